@@ -1,0 +1,232 @@
+/* plp_capi.h -- C ABI of the B200 extreme-point decoder (libplp_b200.so).
+ *
+ * Plain C types only (pointers, sizes, status codes); no exceptions, no exit().
+ * Every entry point returns a plp_status (0 = PLP_OK). The last error message
+ * of the calling thread is available from plp_last_error(NULL); handle-bound
+ * calls also record it on the handle (plp_last_error(handle)).
+ *
+ * Reference interfaces each group replaces (pqant/plp-gpu):
+ *   plp_feas_check_all   FeasibilityBackend::check_all, gpu/plp_common.hpp:326-332
+ *                        (CUDA impl CudaBackend::check_all, gpu/plp_gpu.cu:443-495)
+ *   plp_instance_*       plp::parse / plp::load_instance, gpu/plp_common.hpp:68-151
+ *   plp_run_plain        plp::run with CudaBackend, gpu/plp_gpu.cu:1684-1686 and
+ *                        gpu/plp_common.hpp:471-523 (one feasibility launch per step)
+ *   plp_solve            run_device / run_batch, gpu/plp_gpu.cu:343-412,1395-1474
+ *                        (row k = PyRng(seed + k)), generalised to many instances
+ *   plp_create/submit/.. no reference counterpart: the serving loop
+ *   plp_rng_dump         --rngdump N, gpu/plp_gpu.cu:1479-1536
+ *   plp_fsr_score        plp::stability_score, gpu/plp_common.hpp:393-399
+ *   plp_item_order       plp::item_sequence, gpu/plp_common.hpp:335-351
+ *   plp_to_json / plp_py_repr   plp::to_json / plp::py_repr, gpu/plp_common.hpp:535-610
+ *   plp_selftest         --selftest, gpu/plp_gpu.cpp:43-66
+ */
+#ifndef PLP_CAPI_H
+#define PLP_CAPI_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    PLP_OK = 0,
+    PLP_E_INVALID = 1,      /* bad argument (null pointer, negative size, bad option) */
+    PLP_E_FORMAT = 2,       /* instance text violates the thpack format */
+    PLP_E_CUDA = 3,         /* a CUDA call failed (message names it) */
+    PLP_E_CAPACITY = 4,     /* a size limit of this build was exceeded */
+    PLP_E_BUDGET = 5,       /* request larger than the handle's device-memory budget */
+    PLP_E_TIMEOUT = 6,      /* plp_wait timed out (request still running) */
+    PLP_E_NOT_FOUND = 7,    /* unknown request id */
+    PLP_E_CANCELLED = 8,    /* request was cancelled */
+    PLP_E_PENDING = 9,      /* plp_poll: not finished yet */
+    PLP_E_DEVICE = 10       /* a kernel reported an internal error status */
+} plp_status;
+
+/* ------------------------------------------------------------------------ */
+/* errors                                                                    */
+/* ------------------------------------------------------------------------ */
+typedef struct plp_handle plp_handle;
+/* Message of the last failed call: of the handle when h != NULL, else of the
+ * calling thread. Valid until the next call on the same handle / thread. */
+const char* plp_last_error(const plp_handle* h);
+
+/* ------------------------------------------------------------------------ */
+/* one-step feasibility (the drop-in for FeasibilityBackend::check_all)      */
+/* ------------------------------------------------------------------------ */
+/* Host buffers in and out. bits_out[ci * n_ors + oi] = 1 iff placing
+ * orientation oi = (w, d, h) at candidate ci = (x, y, z) satisfies C2 (inside
+ * L x W x H), C3 (>= 50 % bottom support, FP64 ratio) and C1 (no overlap with
+ * the n_fast placed boxes (x, y, z, x2, y2, z2)). Runs on the calling thread's
+ * CUDA stream and device buffers; thread-safe across threads. */
+int plp_feas_check_all(const int32_t* cand_xyz, int32_t n_cand,
+                       const int32_t* ors_wdh, int32_t n_ors,
+                       const int32_t* fast6, int32_t n_fast,
+                       int32_t L, int32_t W, int32_t H, uint8_t* bits_out);
+
+/* The same on device buffers, enqueued on `stream` (a cudaStream_t, or NULL
+ * for the legacy default stream); no synchronisation. */
+int plp_feas_check_all_dev(const int32_t* d_cand_xyz, int32_t n_cand,
+                           const int32_t* d_ors_wdh, int32_t n_ors,
+                           const int32_t* d_fast6, int32_t n_fast,
+                           int32_t L, int32_t W, int32_t H, uint8_t* d_bits_out,
+                           void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* instances                                                                 */
+/* ------------------------------------------------------------------------ */
+typedef struct plp_instance plp_instance;
+
+/* Parse thpack text holding exactly one instance (P == 1).
+ * PLP_E_FORMAT with the reference parser's message on a violation. */
+int plp_instance_parse(const char* text, size_t len, plp_instance** out);
+/* Parse thpack text with P >= 1 instances; *out receives n instance handles
+ * (free each with plp_instance_free and the array with plp_free). */
+int plp_instance_parse_multi(const char* text, size_t len, plp_instance*** out, int32_t* n);
+int plp_instance_load(const char* path, plp_instance** out);
+/* types7: n_types rows (l, lf, w, wf, h, hf, qty). */
+int plp_instance_from_types(int32_t L, int32_t W, int32_t H, int32_t n_types,
+                            const int32_t* types7, plp_instance** out);
+void plp_instance_free(plp_instance* inst);
+/* L, W, H, n_types, total item count */
+int plp_instance_info(const plp_instance* inst, int32_t* LWH, int32_t* n_types,
+                      int32_t* n_items);
+/* orientation table of one type: up to 6 (w, d, h), dedup'd in parser order */
+int plp_orientations(const plp_instance* inst, int32_t type, int32_t* wdh6x3, int32_t* n);
+/* item sequence on the host: order 0 = volume, 1 = input; ti/copy hold n_items */
+int plp_item_sequence(const plp_instance* inst, int32_t order, int32_t* ti, int32_t* copy);
+void plp_free(void* p);
+
+/* ------------------------------------------------------------------------ */
+/* run options and results                                                   */
+/* ------------------------------------------------------------------------ */
+typedef struct {
+    int64_t seed;         /* restart k uses PyRng(|seed + k|) */
+    int32_t restarts;     /* >= 1 */
+    int32_t passes;       /* >= 1 fixed passes per restart (RNG carried over) */
+    double eps;           /* eps-greedy probability */
+    double theta;         /* acceptance threshold; NaN = no threshold (--no-theta) */
+    int32_t order;        /* 0 = volume, 1 = input */
+    int32_t first_fit;    /* 1 = always the first feasible pair */
+    double mu;            /* friction coefficient (reference default 0.2) */
+    double time_limit_s;  /* < 0: exactly `passes` passes; >= 0: passes until the
+                             wall clock reaches it (plp_run_plain only) */
+    int32_t best_only;    /* 1: copy back the placements of the best restart only
+                             (summaries of every restart are always returned) */
+} plp_run_opts;
+
+void plp_default_opts(plp_run_opts* o);   /* reference CLI defaults */
+
+typedef struct {
+    int32_t n_boxes;
+    int32_t fallback;
+    int64_t volume;
+    double score;
+    int32_t n_passes;
+    int32_t err;          /* 0, or a device status for this restart */
+    int64_t seed;
+    double time_s;
+} plp_summary;
+
+typedef struct plp_result plp_result;   /* results of one instance's restarts */
+
+int32_t plp_result_restarts(const plp_result* r);
+int plp_result_summary(const plp_result* r, int32_t restart, plp_summary* out);
+/* placements as rows (type, x, y, z, w, d, h); n_out receives the count */
+int plp_result_placements(const plp_result* r, int32_t restart, int32_t* rows7,
+                          int32_t cap, int32_t* n_out);
+/* best restart (accepted first, max (volume, n_boxes), earliest on ties) */
+int plp_result_best(const plp_result* r, int32_t* restart, int32_t* fallback);
+/* reference JSON of one restart (plp/solver.py:297-307 layout). Writes at most
+ * cap bytes incl. NUL; *needed receives the full length excl. NUL. */
+int plp_result_json(const plp_result* r, int32_t restart, char* buf, size_t cap, size_t* needed);
+void plp_result_free(plp_result* r);
+/* Reference work of one restart's reported pass, the roofline's algorithmic
+ * unit: aabb_tests = sum over steps of 2 * n_placed * (C2-surviving pairs of
+ * the reference candidate list), pairs = sum of n_cand * n_ors. */
+int plp_result_work(const plp_result* r, int32_t restart, int64_t* aabb_tests, int64_t* pairs);
+
+/* ------------------------------------------------------------------------ */
+/* plain path: host decode loop, one feasibility launch per item step        */
+/* ------------------------------------------------------------------------ */
+int plp_run_plain(const plp_instance* inst, const plp_run_opts* opts, plp_result** out);
+
+/* ------------------------------------------------------------------------ */
+/* handle: device arena, stream, persistent batched solver, serving loop     */
+/* ------------------------------------------------------------------------ */
+/* budget_bytes: device memory the handle may hold for admitted requests
+ * (0 = 100 GB). device: CUDA ordinal. */
+int plp_create(size_t budget_bytes, int32_t device, plp_handle** out);
+void plp_destroy(plp_handle* h);
+
+/* Decoder tile for later solves on this handle: placed-box depth P, live-point
+ * depth C (both per decoder, in shared memory) and decoders per CTA D (1..8);
+ * 0 keeps the current value. Restarts that outgrow the tile are re-run with a
+ * deeper one, so the tile affects speed only, never results. */
+int plp_set_tile(plp_handle* h, int32_t P, int32_t C, int32_t D);
+
+/* Synchronous batched solve: every restart of every instance in one
+ * persistent decoder launch (plus a FSR/selection launch), results copied to
+ * the host. opts holds n_inst entries (or 1 entry shared by all). */
+int plp_solve(plp_handle* h, const plp_instance* const* insts, int32_t n_inst,
+              const plp_run_opts* opts, int32_t n_opts, plp_result** results);
+
+/* Prepared batch: the tables of a solve uploaded once and kept resident, so a
+ * caller can run the device part repeatedly (timing) and fetch results when
+ * it wants them. plp_batch_run is synchronous; device_ms is the CUDA-event
+ * time of all device work of the run, decoder_ms that of the decoder kernel
+ * alone, launches the number of kernels launched. */
+typedef struct plp_batch plp_batch;
+int plp_batch_prepare(plp_handle* h, const plp_instance* const* insts, int32_t n_inst,
+                      const plp_run_opts* opts, int32_t n_opts, plp_batch** out);
+int plp_batch_run(plp_batch* b, double* device_ms, double* decoder_ms, int32_t* launches);
+/* results of the last run (n_inst result objects) */
+int plp_batch_fetch(plp_batch* b, plp_result** results);
+/* bytes the batch copies host->device (tables) and device->host (results) */
+int plp_batch_io_bytes(const plp_batch* b, int64_t* h2d, int64_t* d2h);
+void plp_batch_free(plp_batch* b);
+
+/* Serving: admit a request; it starts as soon as the memory budget allows and
+ * runs concurrently with other admitted requests. */
+int plp_submit(plp_handle* h, const plp_instance* inst, const plp_run_opts* opts,
+               int64_t* request_id);
+/* PLP_OK when finished, PLP_E_PENDING while queued or running */
+int plp_poll(plp_handle* h, int64_t request_id);
+/* block until finished or timeout_ms elapses (< 0: no timeout) */
+int plp_wait(plp_handle* h, int64_t request_id, int64_t timeout_ms);
+/* take the finished result (ownership passes to the caller) */
+int plp_take_result(plp_handle* h, int64_t request_id, plp_result** out);
+int plp_cancel(plp_handle* h, int64_t request_id);
+/* seconds from submit to finish, and to start on the device */
+int plp_request_times(plp_handle* h, int64_t request_id, double* queued_s, double* total_s);
+
+/* ------------------------------------------------------------------------ */
+/* kernel-level hooks (parity tests of the individual device kernels)        */
+/* ------------------------------------------------------------------------ */
+/* device MT19937 (kernel c): for each seed, n_random random() doubles then
+ * n_bits getrandbits(k_bits) values, CPython-exact. */
+int plp_rng_dump(const int64_t* seeds, int32_t n_seeds, int32_t n_random,
+                 int32_t n_bits, int32_t k_bits, double* out_random, uint32_t* out_bits);
+/* the same stream from the host MT19937 (the plain path's generator) */
+int plp_rng_dump_host(const int64_t* seeds, int32_t n_seeds, int32_t n_random,
+                      int32_t n_bits, int32_t k_bits, double* out_random, uint32_t* out_bits);
+/* device FSR (kernel e): packings given as rows (type, x, y, z, w, d, h);
+ * offsets[n_pack + 1] delimit packings. */
+int plp_fsr_score(const int32_t* rows7, const int32_t* offsets, int32_t n_pack, double mu,
+                  double* out_score, double* out_fsr);
+/* device item-order sort (kernel d): per instance sequence of types. */
+int plp_item_order(const plp_instance* const* insts, int32_t n_inst, int32_t order,
+                   int32_t* out_types, int64_t* out_offsets);
+
+/* ------------------------------------------------------------------------ */
+/* host formatting                                                           */
+/* ------------------------------------------------------------------------ */
+int plp_py_repr(double x, char* buf, size_t cap);
+/* the reference --selftest text (RNG + repr blocks); *needed as in plp_result_json */
+int plp_selftest(char* buf, size_t cap, size_t* needed);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PLP_CAPI_H */

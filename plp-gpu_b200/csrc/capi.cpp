@@ -1,0 +1,1493 @@
+// capi.cpp -- C ABI of libplp_b200.so: instances, results, the batched
+// persistent solver, the serving loop and the kernel test hooks.
+//
+// Device memory of a batch comes from the stream-ordered allocator
+// (cudaMallocAsync/cudaFreeAsync) so waves on different streams never force a
+// device-wide synchronisation; the handle's budget bounds the bytes of all
+// batches in flight.
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <climits>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+
+#include "capi_internal.hpp"
+#include "engine.hpp"
+
+using namespace plpb;
+
+// ===========================================================================
+// errors
+// ===========================================================================
+namespace {
+thread_local std::string g_err;
+}
+
+namespace plpb {
+
+int set_error(int code, const std::string& msg) {
+    g_err = msg;
+    return code;
+}
+
+std::string plpb_last() { return g_err; }
+
+int set_cuda_error(const char* what, cudaError_t e) {
+    g_err = std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
+    return PLP_E_CUDA;
+}
+
+double now_seconds() {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+void mt_init_table(uint32_t out[624]) {
+    out[0] = 19650218u;
+    for (uint32_t i = 1; i < 624; i++) out[i] = 1812433253u * (out[i - 1] ^ (out[i - 1] >> 30)) + i;
+}
+
+const uint32_t* device_mt_init(int* status) {
+    static std::mutex mu;
+    static std::map<int, uint32_t*> per_dev;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) { *status = set_cuda_error("cudaGetDevice", e); return nullptr; }
+    std::lock_guard<std::mutex> g(mu);
+    auto it = per_dev.find(dev);
+    if (it != per_dev.end()) { *status = PLP_OK; return it->second; }
+    uint32_t tab[624];
+    mt_init_table(tab);
+    uint32_t* d = nullptr;
+    e = cudaMalloc(&d, sizeof tab);
+    if (e != cudaSuccess) { *status = set_cuda_error("MT init table allocation", e); return nullptr; }
+    e = cudaMemcpy(d, tab, sizeof tab, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) { *status = set_cuda_error("MT init table copy", e); return nullptr; }
+    per_dev[dev] = d;
+    *status = PLP_OK;
+    return d;
+}
+
+}  // namespace plpb
+
+struct plp_handle;
+
+namespace {
+
+std::mutex g_handle_err_mu;
+
+void record(plp_handle* h, int status);
+
+// ===========================================================================
+// batch: device tables + one persistent decoder launch (+ retries)
+// ===========================================================================
+struct TileConfig {
+    int P = 128;       // placed-box tile depth per decoder
+    int C = 384;       // live-point tile depth per decoder
+    int D = 4;         // decoders (warps) per CTA
+};
+
+// Tiles only deepen: a retry that needed a deeper tile is remembered so the
+// next batch of this handle starts there.
+void remember_tile(TileConfig& keep, const TileConfig& used) {
+    if (used.P > keep.P || used.C > keep.C) keep = used;
+}
+
+constexpr int P_MAX = 2048;
+constexpr int C_MAX = 8192;
+
+struct Batch {
+    std::vector<const Instance*> insts;
+    std::vector<plp_run_opts> opts;
+    // host tables
+    std::vector<InstDesc> desc;
+    std::vector<int> steps;
+    std::vector<TypeOrs> types;
+    std::vector<std::vector<TypeOrs>> inst_ors;
+    std::vector<int2> work;
+    long long n_slots = 0, n_places = 0;
+    int max_stride = 1, max_steps = 0;
+    bool multi_pass = false;
+    // device
+    char* d_mem = nullptr;
+    size_t bytes = 0;
+    size_t o_desc, o_steps, o_types, o_work, o_next, o_heads, o_places, o_best, o_scratch, o_gather, o_redo;
+    const uint32_t* mt_init = nullptr;
+    cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+    char* h_flag = nullptr;                // pinned error-flag word
+    std::vector<int2> redo_host;
+    int2* h_redo_stage(size_t n) { redo_host.resize(n); return redo_host.data(); }
+    size_t scratch_bytes = 0;
+    int ctas = 0;
+    TileConfig tile;
+    // host results
+    std::vector<SlotHead> heads;
+    std::vector<int2> best;
+    std::vector<unsigned long long> places;   // all slots, or gathered best per instance
+    bool best_only = false;
+    double t_start = 0, t_end = 0;
+
+    // validate and build the host tables; returns a status
+    int build(const std::vector<const Instance*>& in, const std::vector<plp_run_opts>& op) {
+        insts = in;
+        opts = op;
+        desc.clear(); steps.clear(); types.clear(); work.clear(); inst_ors.clear();
+        n_slots = 0; n_places = 0; max_stride = 1; max_steps = 0; multi_pass = false;
+        best_only = true;
+        for (size_t i = 0; i < in.size(); i++) {
+            const Instance& I = *in[i];
+            const plp_run_opts& o = op[i];
+            if (o.restarts < 1 || o.passes < 1)
+                return set_error(PLP_E_INVALID, "restarts and passes must be >= 1");
+            if (o.order != 0 && o.order != 1) return set_error(PLP_E_INVALID, "order must be 0 or 1");
+            int xb = 0, yb = 0, zb = 0;
+            for (int v = I.L; v; v >>= 1) xb++;
+            for (int v = I.W; v; v >>= 1) yb++;
+            for (int v = I.H; v; v >>= 1) zb++;
+            if (xb + yb + zb > 32 || I.L >= 65536 || I.W >= 65536 || I.H >= 65536)
+                return set_error(PLP_E_CAPACITY,
+                                 "container too large for 32-bit point keys (bit lengths of L, W, H "
+                                 "must sum to <= 32)");
+            if ((int)I.types.size() >= 8192)
+                return set_error(PLP_E_CAPACITY, "more than 8191 box types");
+            const std::vector<int> seq = item_sequence(I, o.order);
+            InstDesc d{};
+            d.L = I.L; d.W = I.W; d.H = I.H;
+            d.n_steps = (int)seq.size();
+            d.step_off = (int)steps.size();
+            d.type_off = (int)types.size();
+            d.xb = xb; d.yb = yb;
+            d.restarts = o.restarts;
+            d.slot_base = (int)n_slots;
+            d.place_stride = std::max(1, d.n_steps);
+            d.passes = o.passes;
+            d.place_off = n_places;
+            d.seed = o.seed;
+            d.eps = o.eps;
+            d.has_theta = std::isnan(o.theta) ? 0 : 1;
+            d.theta = d.has_theta ? o.theta : 0.0;
+            d.mu = o.mu;
+            d.first_fit = o.first_fit ? 1 : 0;
+            desc.push_back(d);
+            steps.insert(steps.end(), seq.begin(), seq.end());
+            std::vector<TypeOrs> ot;
+            for (const auto& t : I.types) {
+                TypeOrs to{};
+                const auto v = orientations(t);
+                to.n = (int)v.size();
+                for (int k = 0; k < to.n; k++) { to.w[k] = v[k][0]; to.d[k] = v[k][1]; to.h[k] = v[k][2]; }
+                ot.push_back(to);
+                types.push_back(to);
+            }
+            inst_ors.push_back(std::move(ot));
+            n_slots += o.restarts;
+            n_places += (long long)o.restarts * d.place_stride;
+            max_stride = std::max(max_stride, d.place_stride);
+            max_steps = std::max(max_steps, d.n_steps);
+            multi_pass = multi_pass || o.passes > 1;
+            best_only = best_only && o.best_only;
+        }
+        if (n_slots > INT_MAX / 2) return set_error(PLP_E_CAPACITY, "too many restarts in one batch");
+        // longest instances first (dynamic scheduling then balances the tail)
+        std::vector<int> order(in.size());
+        for (size_t i = 0; i < in.size(); i++) order[i] = (int)i;
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+            return desc[a].n_steps * desc[a].passes > desc[b].n_steps * desc[b].passes;
+        });
+        work.reserve(n_slots);
+        for (int i : order)
+            for (int r = 0; r < desc[i].restarts; r++) work.push_back(make_int2(i, r));
+        return PLP_OK;
+    }
+
+    static size_t al(size_t v) { return (v + 255) & ~size_t(255); }
+
+    void plan(int sms, const TileConfig& t) {
+        tile = t;
+        int occ = 1;
+        if (decoder_occupancy(t.P, t.C, t.D, &occ) != cudaSuccess || occ < 1) occ = 1;
+        const long long need = (n_slots + t.D - 1) / t.D;
+        ctas = (int)std::max(1LL, std::min<long long>(need, (long long)sms * occ));
+        scratch_bytes = multi_pass ? (size_t)ctas * t.D * max_stride * 8 : 0;
+        size_t o = 0;
+        o_desc = o;    o = al(o + desc.size() * sizeof(InstDesc));
+        o_steps = o;   o = al(o + std::max<size_t>(1, steps.size()) * sizeof(int));
+        o_types = o;   o = al(o + std::max<size_t>(1, types.size()) * sizeof(TypeOrs));
+        o_work = o;    o = al(o + work.size() * sizeof(int2));
+        o_next = o;    o = al(o + 16);
+        o_heads = o;   o = al(o + n_slots * sizeof(SlotHead));
+        o_places = o;  o = al(o + std::max<long long>(1, n_places) * 8);
+        o_best = o;    o = al(o + desc.size() * sizeof(int2));
+        o_gather = o;  o = al(o + desc.size() * (size_t)max_stride * 8);
+        o_scratch = o; o = al(o + std::max<size_t>(8, scratch_bytes));
+        o_redo = o;    o = al(o + work.size() * sizeof(int2));
+        bytes = o;
+    }
+
+    size_t upload_bytes() const { return o_next; }   // desc .. work are contiguous at the front
+};
+
+// pinned staging buffer per thread (grows)
+struct Pinned {
+    char* p = nullptr;
+    size_t cap = 0;
+    ~Pinned() { if (p) cudaFreeHost(p); }
+    cudaError_t ensure(size_t n) {
+        if (n <= cap) return cudaSuccess;
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        cap = 0;
+        size_t c = 1 << 20;
+        while (c < n) c <<= 1;
+        cudaError_t e = cudaMallocHost(&p, c);
+        if (e == cudaSuccess) cap = c;
+        return e;
+    }
+};
+
+}  // namespace
+
+// gather of the best restart's placements (decoder.cu)
+namespace plpb {
+cudaError_t launch_gather_best(const InstDesc* inst, int n_inst, const int2* best,
+                               const unsigned long long* places, unsigned long long* out,
+                               int out_stride, cudaStream_t st);
+}
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// batch stages: prepare (tables to the device), execute (decode + select,
+// CUDA-event timed, capacity retries), fetch (results to the host), release.
+// Device memory comes from the stream-ordered pool.
+// ---------------------------------------------------------------------------
+struct ExecStats {
+    double device_ms = 0, decoder_ms = 0;
+    int launches = 0;
+};
+
+int batch_release(Batch& b, cudaStream_t st) {
+    cudaError_t e = cudaSuccess;
+    if (b.d_mem) e = cudaFreeAsync(b.d_mem, st);
+    b.d_mem = nullptr;
+    cudaError_t e2 = cudaStreamSynchronize(st);
+    for (auto& ev : b.ev)
+        if (ev) { cudaEventDestroy(ev); ev = nullptr; }
+    if (b.h_flag) { cudaFreeHost(b.h_flag); b.h_flag = nullptr; }
+    if (e != cudaSuccess) return set_cuda_error("batch free", e);
+    if (e2 != cudaSuccess) return set_cuda_error("batch completion", e2);
+    return PLP_OK;
+}
+
+int batch_prepare(Batch& b, cudaStream_t st, Pinned& pin, int sms, const TileConfig& tc) {
+    int status = PLP_OK;
+    b.mt_init = device_mt_init(&status);
+    if (!b.mt_init) return status;
+    b.plan(sms, tc);
+    auto fail = [&](const char* what, cudaError_t err) {
+        const int s = set_cuda_error(what, err);
+        std::string keep = plpb_last();
+        batch_release(b, st);
+        set_error(s, keep);
+        return s;
+    };
+    cudaError_t e;
+    for (auto& ev : b.ev) {
+        e = cudaEventCreate(&ev);
+        if (e != cudaSuccess) return fail("event creation", e);
+    }
+    e = cudaMallocHost(&b.h_flag, 64);
+    if (e != cudaSuccess) return fail("pinned flag", e);
+    e = cudaMallocAsync(&b.d_mem, b.bytes, st);
+    if (e != cudaSuccess) return fail("batch allocation", e);
+    const size_t up = b.upload_bytes();
+    e = pin.ensure(std::max(up, (size_t)1));
+    if (e != cudaSuccess) return fail("pinned staging", e);
+    std::memcpy(pin.p + b.o_desc, b.desc.data(), b.desc.size() * sizeof(InstDesc));
+    std::memcpy(pin.p + b.o_steps, b.steps.data(), b.steps.size() * sizeof(int));
+    std::memcpy(pin.p + b.o_types, b.types.data(), b.types.size() * sizeof(TypeOrs));
+    std::memcpy(pin.p + b.o_work, b.work.data(), b.work.size() * sizeof(int2));
+    e = cudaMemcpyAsync(b.d_mem, pin.p, up, cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return fail("batch upload", e);
+    // the staging buffer is reused by the next batch of this thread
+    e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return fail("batch upload", e);
+    return PLP_OK;
+}
+
+static DecodeLaunch make_launch(const Batch& b, const TileConfig& t, const int2* work, int n_work, int sms) {
+    DecodeLaunch L{};
+    L.inst = reinterpret_cast<const InstDesc*>(b.d_mem + b.o_desc);
+    L.step_type = reinterpret_cast<const int*>(b.d_mem + b.o_steps);
+    L.types = reinterpret_cast<const TypeOrs*>(b.d_mem + b.o_types);
+    L.work = work;
+    L.n_work = n_work;
+    L.work_next = reinterpret_cast<int*>(b.d_mem + b.o_next);
+    L.err_flag = reinterpret_cast<int*>(b.d_mem + b.o_next + 8);
+    L.heads = reinterpret_cast<SlotHead*>(b.d_mem + b.o_heads);
+    L.places = reinterpret_cast<unsigned long long*>(b.d_mem + b.o_places);
+    L.scratch = reinterpret_cast<unsigned long long*>(b.d_mem + b.o_scratch);
+    L.mt_init = b.mt_init;
+    L.P = t.P;
+    L.C = t.C;
+    L.decoders_per_cta = t.D;
+    int occ = 1;
+    if (decoder_occupancy(t.P, t.C, t.D, &occ) != cudaSuccess || occ < 1) occ = 1;
+    L.ctas = (int)std::max<long long>(1, std::min<long long>((n_work + t.D - 1) / t.D, (long long)sms * occ));
+    // multi-pass scratch holds one placement row per resident decoder
+    if (b.multi_pass) {
+        const size_t per_cta = (size_t)t.D * b.max_stride * 8;
+        L.ctas = (int)std::max<size_t>(1, std::min<size_t>((size_t)L.ctas, b.scratch_bytes / per_cta));
+    }
+    return L;
+}
+
+// tile: in = tile to use, out = tile that succeeded (deeper after retries)
+int batch_execute(Batch& b, cudaStream_t st, int sms, TileConfig& tile, ExecStats* xs) {
+    auto fail = [&](const char* what, cudaError_t err) {
+        const int s = set_cuda_error(what, err);
+        std::string keep = plpb_last();
+        batch_release(b, st);
+        set_error(s, keep);
+        return s;
+    };
+    ExecStats x;
+    TileConfig t = tile;
+    const int2* d_work = reinterpret_cast<const int2*>(b.d_mem + b.o_work);
+    int* d_flag = reinterpret_cast<int*>(b.d_mem + b.o_next + 8);
+    cudaError_t e = cudaMemsetAsync(d_flag, 0, 8, st);
+    if (e != cudaSuccess) return fail("flag reset", e);
+    e = cudaEventRecord(b.ev[0], st);
+    if (e == cudaSuccess) e = launch_decoder(make_launch(b, t, d_work, (int)b.work.size(), sms), st);
+    if (e == cudaSuccess) e = cudaEventRecord(b.ev[1], st);
+    if (e != cudaSuccess) return fail("decoder launch", e);
+    x.launches++;
+    e = cudaMemcpyAsync(b.h_flag, d_flag, 4, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return fail("decoder", e);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, b.ev[0], b.ev[1]);
+    x.decoder_ms = ms;
+    // capacity retries: restarts whose live points or boxes outgrew the tile
+    // run again with a deeper tile (same slots, so results land in place)
+    for (int attempt = 0; *reinterpret_cast<volatile int*>(b.h_flag) != 0; attempt++) {
+        if (*reinterpret_cast<volatile int*>(b.h_flag) & (1 << ERR_RNG)) {
+            batch_release(b, st);
+            return set_error(PLP_E_DEVICE, "decoder reported an RNG rejection-bound error");
+        }
+        b.heads.resize(b.n_slots);
+        e = cudaMemcpyAsync(b.heads.data(), b.d_mem + b.o_heads, b.n_slots * sizeof(SlotHead),
+                            cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return fail("head copy", e);
+        std::vector<int2> redo;
+        bool grow_p = false, grow_c = false;
+        for (const int2& w : b.work) {
+            const SlotHead& h = b.heads[b.desc[w.x].slot_base + w.y];
+            if (h.err == ERR_BOX_CAP) { grow_p = true; redo.push_back(w); }
+            else if (h.err == ERR_CAND_CAP) { grow_c = true; redo.push_back(w); }
+        }
+        if (redo.empty() || attempt == 6) {
+            batch_release(b, st);
+            return set_error(PLP_E_CAPACITY, "decoder tile capacity exceeded after retries");
+        }
+        if (grow_p) t.P = std::min(P_MAX, std::max(t.P * 2, 32));
+        if (grow_c) t.C = std::min(C_MAX, t.C * 2);
+        // deeper tiles: fewer decoders per CTA keeps one CTA within 227 KB
+        while (t.D > 1 && decoder_smem_bytes(t.P, t.C) * t.D > 200 * 1024) t.D >>= 1;
+        if (decoder_smem_bytes(t.P, t.C) > 227 * 1024) {
+            batch_release(b, st);
+            return set_error(PLP_E_CAPACITY, "instance needs a larger tile than shared memory holds");
+        }
+        std::memcpy(b.h_redo_stage(redo.size()), redo.data(), redo.size() * sizeof(int2));
+        int2* d_redo = reinterpret_cast<int2*>(b.d_mem + b.o_redo);
+        e = cudaMemcpyAsync(d_redo, b.redo_host.data(), redo.size() * sizeof(int2), cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) e = cudaMemsetAsync(d_flag, 0, 8, st);
+        if (e == cudaSuccess) e = launch_decoder(make_launch(b, t, d_redo, (int)redo.size(), sms), st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(b.h_flag, d_flag, 4, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return fail("decoder relaunch", e);
+        x.launches++;
+    }
+    int2* d_best = reinterpret_cast<int2*>(b.d_mem + b.o_best);
+    const InstDesc* d_inst = reinterpret_cast<const InstDesc*>(b.d_mem + b.o_desc);
+    const SlotHead* d_heads = reinterpret_cast<const SlotHead*>(b.d_mem + b.o_heads);
+    e = launch_select_best(d_inst, (int)b.desc.size(), d_heads, d_best, st);
+    if (e != cudaSuccess) return fail("select launch", e);
+    x.launches++;
+    if (b.best_only) {
+        unsigned long long* d_g = reinterpret_cast<unsigned long long*>(b.d_mem + b.o_gather);
+        e = launch_gather_best(d_inst, (int)b.desc.size(), d_best,
+                               reinterpret_cast<const unsigned long long*>(b.d_mem + b.o_places), d_g,
+                               b.max_stride, st);
+        if (e != cudaSuccess) return fail("gather launch", e);
+        x.launches++;
+    }
+    e = cudaEventRecord(b.ev[2], st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return fail("select", e);
+    cudaEventElapsedTime(&ms, b.ev[0], b.ev[2]);
+    x.device_ms = ms;
+    tile = t;
+    if (xs) *xs = x;
+    return PLP_OK;
+}
+
+int batch_fetch(Batch& b, cudaStream_t st) {
+    b.heads.resize(b.n_slots);
+    b.best.resize(b.desc.size());
+    cudaError_t e = cudaMemcpyAsync(b.heads.data(), b.d_mem + b.o_heads, b.n_slots * sizeof(SlotHead),
+                                    cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(b.best.data(), b.d_mem + b.o_best, b.desc.size() * sizeof(int2),
+                            cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) {
+        if (b.best_only) {
+            b.places.resize(b.desc.size() * (size_t)b.max_stride);
+            e = cudaMemcpyAsync(b.places.data(), b.d_mem + b.o_gather, b.places.size() * 8,
+                                cudaMemcpyDeviceToHost, st);
+        } else {
+            b.places.resize((size_t)std::max<long long>(1, b.n_places));
+            e = cudaMemcpyAsync(b.places.data(), b.d_mem + b.o_places, b.n_places * 8,
+                                cudaMemcpyDeviceToHost, st);
+        }
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+        const int s = set_cuda_error("result copy", e);
+        std::string keep = plpb_last();
+        batch_release(b, st);
+        set_error(s, keep);
+        return s;
+    }
+    return PLP_OK;
+}
+
+// bytes copied host->device per execution and device->host per fetch
+size_t batch_h2d_bytes(const Batch& b) { return b.upload_bytes(); }
+size_t batch_d2h_bytes(const Batch& b) {
+    return b.n_slots * sizeof(SlotHead) + b.desc.size() * sizeof(int2) +
+           (b.best_only ? b.desc.size() * (size_t)b.max_stride * 8 : (size_t)b.n_places * 8);
+}
+
+// full synchronous run used by plp_solve and the serving workers
+int run_batch(Batch& b, cudaStream_t st, Pinned& pin, int sms, TileConfig& tile) {
+    int s = batch_prepare(b, st, pin, sms, tile);
+    if (s != PLP_OK) return s;
+    s = batch_execute(b, st, sms, tile, nullptr);
+    if (s != PLP_OK) return s;
+    s = batch_fetch(b, st);
+    if (s != PLP_OK) return s;
+    return batch_release(b, st);
+}
+
+// Builds the per-instance result objects of a finished batch.
+std::vector<plp_result*> collect(const Batch& b, double time_s) {
+    std::vector<plp_result*> out;
+    for (size_t i = 0; i < b.desc.size(); i++) {
+        const InstDesc& d = b.desc[i];
+        auto* r = new plp_result;
+        r->restarts = d.restarts;
+        r->stride = d.place_stride;
+        r->ors = b.inst_ors[i];
+        r->L = d.L; r->W = d.W; r->H = d.H;
+        r->steps.assign(b.steps.begin() + d.step_off, b.steps.begin() + d.step_off + d.n_steps);
+        r->summ.resize(d.restarts);
+        for (int k = 0; k < d.restarts; k++) {
+            const SlotHead& h = b.heads[d.slot_base + k];
+            plp_summary& s = r->summ[k];
+            s.n_boxes = h.n_boxes;
+            s.fallback = h.fallback;
+            s.volume = h.volume;
+            s.score = h.score;
+            s.n_passes = h.n_passes;
+            s.err = h.err;
+            s.seed = d.seed + k;
+            s.time_s = time_s;
+        }
+        r->best = b.best[i].x;
+        r->best_fallback = b.best[i].y;
+        r->packed_slot.assign(d.restarts, -1);
+        if (b.best_only) {
+            r->packed.assign(b.places.begin() + (long long)i * b.max_stride,
+                             b.places.begin() + (long long)i * b.max_stride + d.place_stride);
+            if (r->best >= 0) r->packed_slot[r->best] = 0;
+        } else {
+            r->packed.assign(b.places.begin() + d.place_off,
+                             b.places.begin() + d.place_off + (long long)d.restarts * d.place_stride);
+            for (int k = 0; k < d.restarts; k++) r->packed_slot[k] = k;
+        }
+        out.push_back(r);
+    }
+    return out;
+}
+
+}  // namespace
+
+// ===========================================================================
+// handle: budget, streams, serving loop
+// ===========================================================================
+struct Request {
+    int64_t id;
+    Instance inst;
+    plp_run_opts opts;
+    size_t bytes = 0;
+    int status = PLP_E_PENDING;   // PLP_E_PENDING until finished
+    bool running = false, cancelled = false;
+    std::string err;
+    plp_result* result = nullptr;
+    double t_submit = 0, t_start = 0, t_done = 0;
+};
+
+struct plp_handle {
+    int device = 0;
+    int sms = 148;
+    size_t budget = 0;
+    size_t in_use = 0;
+    TileConfig tile;
+    std::string err;
+    std::mutex mu;
+    std::condition_variable cv;       // request state changes
+    std::condition_variable cv_sched; // work for the scheduler
+    std::deque<int64_t> queue;
+    std::unordered_map<int64_t, std::unique_ptr<Request>> reqs;
+    int64_t next_id = 1;
+    bool stop = false;
+    int n_workers = 4;
+    int busy_workers = 0;
+    std::vector<std::thread> workers;
+    std::vector<cudaStream_t> streams;
+    // synchronous solves
+    cudaStream_t sync_stream = nullptr;
+    std::mutex sync_mu;
+    Pinned sync_pin;
+};
+
+namespace {
+
+void record(plp_handle* h, int status) {
+    if (h && status != PLP_OK && status != PLP_E_PENDING) {
+        std::lock_guard<std::mutex> g(g_handle_err_mu);
+        h->err = g_err;
+    }
+}
+
+// rough device bytes of one request (tables + results + scratch share)
+size_t request_bytes(const Instance& I, const plp_run_opts& o) {
+    const size_t steps = (size_t)std::max(1, I.n_items());
+    return 4096 + I.types.size() * sizeof(TypeOrs) + steps * 4 +
+           (size_t)o.restarts * (sizeof(int2) + sizeof(SlotHead) + steps * 8) +
+           (o.passes > 1 ? (size_t)148 * 64 * steps * 8 : 0);
+}
+
+void worker_main(plp_handle* h, int wi) {
+    cudaSetDevice(h->device);
+    Pinned pin;
+    cudaStream_t st = h->streams[wi];
+    for (;;) {
+        std::vector<Request*> wave;
+        size_t wave_bytes = 0;
+        {
+            std::unique_lock<std::mutex> lk(h->mu);
+            h->cv_sched.wait(lk, [&] {
+                if (h->stop) return true;
+                if (h->queue.empty()) return false;
+                auto it = h->reqs.find(h->queue.front());
+                if (it == h->reqs.end()) return true;
+                Request* r = it->second.get();
+                return r->cancelled || h->in_use + r->bytes <= h->budget;
+            });
+            if (h->stop) return;
+            // admit queued requests in arrival order while the budget allows
+            while (!h->queue.empty()) {
+                auto it = h->reqs.find(h->queue.front());
+                if (it == h->reqs.end() || it->second->cancelled) {
+                    h->queue.pop_front();
+                    continue;
+                }
+                Request* r = it->second.get();
+                if (h->in_use + wave_bytes + r->bytes > h->budget) break;
+                wave_bytes += r->bytes;
+                r->running = true;
+                r->t_start = now_seconds();
+                wave.push_back(r);
+                h->queue.pop_front();
+                if (wave.size() >= 4096) break;
+            }
+            h->in_use += wave_bytes;
+            h->busy_workers++;
+        }
+        if (wave.empty()) {
+            std::lock_guard<std::mutex> lk(h->mu);
+            h->busy_workers--;
+            continue;
+        }
+        Batch b;
+        std::vector<const Instance*> in;
+        std::vector<plp_run_opts> op;
+        for (Request* r : wave) {
+            in.push_back(&r->inst);
+            op.push_back(r->opts);
+        }
+        const double t0 = now_seconds();
+        int s = b.build(in, op);
+        TileConfig tile;
+        {
+            std::lock_guard<std::mutex> lk(h->mu);
+            tile = h->tile;
+        }
+        if (s == PLP_OK) s = run_batch(b, st, pin, h->sms, tile);
+        if (s == PLP_OK) {
+            std::lock_guard<std::mutex> lk(h->mu);
+            remember_tile(h->tile, tile);
+        }
+        std::vector<plp_result*> res;
+        if (s == PLP_OK) res = collect(b, now_seconds() - t0);
+        const std::string msg = s == PLP_OK ? "" : g_err;
+        {
+            std::lock_guard<std::mutex> lk(h->mu);
+            const double t = now_seconds();
+            for (size_t i = 0; i < wave.size(); i++) {
+                Request* r = wave[i];
+                r->running = false;
+                r->t_done = t;
+                if (s == PLP_OK) {
+                    r->result = res[i];
+                    r->status = r->cancelled ? PLP_E_CANCELLED : PLP_OK;
+                } else {
+                    r->status = s;
+                    r->err = msg;
+                }
+            }
+            h->in_use -= wave_bytes;
+            h->busy_workers--;
+        }
+        h->cv.notify_all();
+        h->cv_sched.notify_all();
+    }
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+const char* plp_last_error(const plp_handle* h) {
+    if (h) return h->err.c_str();
+    return g_err.c_str();
+}
+
+void plp_free(void* p) { free(p); }
+
+void plp_default_opts(plp_run_opts* o) {
+    if (!o) return;
+    o->seed = 0;
+    o->restarts = 1;
+    o->passes = 1;
+    o->eps = 0.3;
+    o->theta = 0.9;
+    o->order = 0;
+    o->first_fit = 0;
+    o->mu = 0.2;
+    o->time_limit_s = -1.0;
+    o->best_only = 0;
+}
+
+// ---- instances -----------------------------------------------------------
+int plp_instance_parse_multi(const char* text, size_t len, plp_instance*** out, int32_t* n) {
+    if (!text || !out || !n) return set_error(PLP_E_INVALID, "plp_instance_parse_multi: null argument");
+    try {
+        auto v = parse_thpack(std::string(text, len));
+        auto** arr = (plp_instance**)malloc(sizeof(plp_instance*) * v.size());
+        for (size_t i = 0; i < v.size(); i++) arr[i] = new plp_instance{std::move(v[i])};
+        *out = arr;
+        *n = (int32_t)v.size();
+        return PLP_OK;
+    } catch (const FormatError& e) {
+        return set_error(PLP_E_FORMAT, e.what());
+    }
+}
+
+int plp_instance_parse(const char* text, size_t len, plp_instance** out) {
+    if (!text || !out) return set_error(PLP_E_INVALID, "plp_instance_parse: null argument");
+    try {
+        auto v = parse_thpack(std::string(text, len));
+        if (v.size() != 1)
+            return set_error(PLP_E_FORMAT, "expected exactly 1 instance, got " + std::to_string(v.size()));
+        *out = new plp_instance{std::move(v[0])};
+        return PLP_OK;
+    } catch (const FormatError& e) {
+        return set_error(PLP_E_FORMAT, e.what());
+    }
+}
+
+int plp_instance_load(const char* path, plp_instance** out) {
+    if (!path || !out) return set_error(PLP_E_INVALID, "plp_instance_load: null argument");
+    try {
+        *out = new plp_instance{load_single(path)};
+        return PLP_OK;
+    } catch (const FormatError& e) {
+        return set_error(PLP_E_FORMAT, e.what());
+    }
+}
+
+int plp_instance_from_types(int32_t L, int32_t W, int32_t H, int32_t n_types, const int32_t* t7,
+                            plp_instance** out) {
+    if (!out || n_types < 0 || (n_types && !t7))
+        return set_error(PLP_E_INVALID, "plp_instance_from_types: bad argument");
+    if (L <= 0 || W <= 0 || H <= 0) return set_error(PLP_E_FORMAT, "container dimensions must be positive");
+    Instance I;
+    I.L = L; I.W = W; I.H = H;
+    for (int i = 0; i < n_types; i++) {
+        const int32_t* r = t7 + 7 * i;
+        if (r[0] <= 0 || r[2] <= 0 || r[4] <= 0)
+            return set_error(PLP_E_FORMAT, "item dimensions must be positive");
+        if ((r[1] | r[3] | r[5]) & ~1) return set_error(PLP_E_FORMAT, "orientation flags must be 0/1");
+        if (r[6] < 0) return set_error(PLP_E_FORMAT, "item qty must be >= 0");
+        BoxType b;
+        b.l = r[0]; b.lf = r[1]; b.w = r[2]; b.wf = r[3]; b.h = r[4]; b.hf = r[5]; b.qty = r[6];
+        I.types.push_back(b);
+    }
+    *out = new plp_instance{std::move(I)};
+    return PLP_OK;
+}
+
+void plp_instance_free(plp_instance* inst) { delete inst; }
+
+int plp_instance_info(const plp_instance* in, int32_t* LWH, int32_t* n_types, int32_t* n_items) {
+    if (!in) return set_error(PLP_E_INVALID, "plp_instance_info: null instance");
+    if (LWH) { LWH[0] = in->inst.L; LWH[1] = in->inst.W; LWH[2] = in->inst.H; }
+    if (n_types) *n_types = (int32_t)in->inst.types.size();
+    if (n_items) *n_items = in->inst.n_items();
+    return PLP_OK;
+}
+
+int plp_orientations(const plp_instance* in, int32_t type, int32_t* wdh, int32_t* n) {
+    if (!in || !wdh || !n) return set_error(PLP_E_INVALID, "plp_orientations: null argument");
+    if (type < 0 || type >= (int)in->inst.types.size())
+        return set_error(PLP_E_INVALID, "plp_orientations: type out of range");
+    const auto v = orientations(in->inst.types[type]);
+    for (size_t i = 0; i < v.size(); i++)
+        for (int k = 0; k < 3; k++) wdh[3 * i + k] = v[i][k];
+    *n = (int32_t)v.size();
+    return PLP_OK;
+}
+
+int plp_item_sequence(const plp_instance* in, int32_t order, int32_t* ti, int32_t* copy) {
+    if (!in || !ti) return set_error(PLP_E_INVALID, "plp_item_sequence: null argument");
+    if (order != 0 && order != 1) return set_error(PLP_E_INVALID, "unknown order");
+    const auto seq = item_sequence(in->inst, order);
+    std::vector<int> seen(in->inst.types.size(), 0);
+    for (size_t i = 0; i < seq.size(); i++) {
+        ti[i] = seq[i];
+        if (copy) copy[i] = seen[seq[i]]++;
+    }
+    return PLP_OK;
+}
+
+// ---- results --------------------------------------------------------------
+int32_t plp_result_restarts(const plp_result* r) { return r ? r->restarts : 0; }
+
+int plp_result_summary(const plp_result* r, int32_t k, plp_summary* out) {
+    if (!r || !out) return set_error(PLP_E_INVALID, "plp_result_summary: null argument");
+    if (k < 0 || k >= r->restarts) return set_error(PLP_E_INVALID, "restart out of range");
+    *out = r->summ[k];
+    return PLP_OK;
+}
+
+static int expand(const plp_result* r, int k, std::vector<Placement>& v) {
+    v.clear();
+    if (!r->row_off.empty()) {
+        v.assign(r->rows.begin() + r->row_off[k], r->rows.begin() + r->row_off[k + 1]);
+        return PLP_OK;
+    }
+    const int slot = r->packed_slot[k];
+    if (slot < 0) return set_error(PLP_E_NOT_FOUND, "placements of this restart were not kept (best_only)");
+    const int n = r->summ[k].n_boxes;
+    for (int i = 0; i < n; i++) {
+        int x, y, z, oi, t;
+        unpack_place(r->packed[(size_t)slot * r->stride + i], x, y, z, oi, t);
+        const TypeOrs& o = r->ors[t];
+        v.push_back({t, x, y, z, o.w[oi], o.d[oi], o.h[oi]});
+    }
+    return PLP_OK;
+}
+
+int plp_result_placements(const plp_result* r, int32_t k, int32_t* rows7, int32_t cap, int32_t* n_out) {
+    if (!r || !n_out) return set_error(PLP_E_INVALID, "plp_result_placements: null argument");
+    if (k < 0 || k >= r->restarts) return set_error(PLP_E_INVALID, "restart out of range");
+    std::vector<Placement> v;
+    int s = expand(r, k, v);
+    if (s != PLP_OK) return s;
+    *n_out = (int32_t)v.size();
+    if (!rows7) return PLP_OK;
+    if (cap < (int)v.size()) return set_error(PLP_E_INVALID, "plp_result_placements: buffer too small");
+    for (size_t i = 0; i < v.size(); i++) {
+        int32_t* q = rows7 + 7 * i;
+        q[0] = v[i].type; q[1] = v[i].x; q[2] = v[i].y; q[3] = v[i].z;
+        q[4] = v[i].w; q[5] = v[i].d; q[6] = v[i].h;
+    }
+    return PLP_OK;
+}
+
+int plp_result_best(const plp_result* r, int32_t* restart, int32_t* fallback) {
+    if (!r) return set_error(PLP_E_INVALID, "plp_result_best: null result");
+    if (restart) *restart = r->best;
+    if (fallback) *fallback = r->best_fallback;
+    return PLP_OK;
+}
+
+int plp_result_json(const plp_result* r, int32_t k, char* buf, size_t cap, size_t* needed) {
+    if (!r) return set_error(PLP_E_INVALID, "plp_result_json: null result");
+    if (k < 0 || k >= r->restarts) return set_error(PLP_E_INVALID, "restart out of range");
+    std::vector<Placement> v;
+    int s = expand(r, k, v);
+    if (s != PLP_OK) return s;
+    const plp_summary& S = r->summ[k];
+    RunSummary rs;
+    rs.n_boxes = S.n_boxes;
+    rs.volume = S.volume;
+    rs.score = S.score;
+    rs.fallback = S.fallback != 0;
+    rs.n_passes = S.n_passes;
+    rs.time_s = S.time_s;
+    rs.seed = S.seed;
+    const std::string js = to_json(rs, v);
+    if (needed) *needed = js.size();
+    if (buf && cap) {
+        const size_t n = std::min(cap - 1, js.size());
+        std::memcpy(buf, js.data(), n);
+        buf[n] = '\0';
+    }
+    return PLP_OK;
+}
+
+void plp_result_free(plp_result* r) { delete r; }
+
+// ---- plain path -----------------------------------------------------------
+int plp_run_plain(const plp_instance* inst, const plp_run_opts* opts, plp_result** out) {
+    if (!inst || !opts || !out) return set_error(PLP_E_INVALID, "plp_run_plain: null argument");
+    if (opts->restarts < 1 || (opts->time_limit_s < 0 && opts->passes < 1))
+        return set_error(PLP_E_INVALID, "restarts and passes must be >= 1");
+    if (opts->order != 0 && opts->order != 1) return set_error(PLP_E_INVALID, "order must be 0 or 1");
+    std::vector<RunSummary> summ;
+    std::vector<std::vector<Placement>> pl;
+    int s = run_plain(inst->inst, *opts, summ, pl);
+    if (s != PLP_OK) return s;
+    auto* r = new plp_result;
+    r->restarts = opts->restarts;
+    r->row_off.push_back(0);
+    r->L = inst->inst.L; r->W = inst->inst.W; r->H = inst->inst.H;
+    r->steps = item_sequence(inst->inst, opts->order);
+    for (const auto& t : inst->inst.types) {
+        TypeOrs to{};
+        const auto v = orientations(t);
+        to.n = (int)v.size();
+        for (int k = 0; k < to.n; k++) { to.w[k] = v[k][0]; to.d[k] = v[k][1]; to.h[k] = v[k][2]; }
+        r->ors.push_back(to);
+    }
+    for (int k = 0; k < opts->restarts; k++) {
+        plp_summary ps{};
+        ps.n_boxes = summ[k].n_boxes;
+        ps.fallback = summ[k].fallback;
+        ps.volume = summ[k].volume;
+        ps.score = summ[k].score;
+        ps.n_passes = summ[k].n_passes;
+        ps.seed = summ[k].seed;
+        ps.time_s = summ[k].time_s;
+        r->summ.push_back(ps);
+        r->rows.insert(r->rows.end(), pl[k].begin(), pl[k].end());
+        r->row_off.push_back((long long)r->rows.size());
+    }
+    // best restart: accepted first, max (volume, n), earliest on ties
+    for (int k = 0; k < r->restarts; k++) {
+        const plp_summary& a = r->summ[k];
+        if (r->best < 0) { r->best = k; continue; }
+        const plp_summary& b = r->summ[r->best];
+        const int aa = !a.fallback, ba = !b.fallback;
+        if (aa != ba ? aa > ba : (a.volume != b.volume ? a.volume > b.volume : a.n_boxes > b.n_boxes))
+            r->best = k;
+    }
+    r->best_fallback = r->best >= 0 ? r->summ[r->best].fallback : 1;
+    *out = r;
+    return PLP_OK;
+}
+
+// ---- handle ---------------------------------------------------------------
+int plp_create(size_t budget_bytes, int32_t device, plp_handle** out) {
+    if (!out) return set_error(PLP_E_INVALID, "plp_create: null argument");
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess) return set_cuda_error("cudaGetDeviceCount", e);
+    if (device < 0 || device >= n) return set_error(PLP_E_INVALID, "plp_create: no such device");
+    e = cudaSetDevice(device);
+    if (e != cudaSuccess) return set_cuda_error("cudaSetDevice", e);
+    auto* h = new plp_handle;
+    h->device = device;
+    h->budget = budget_bytes ? budget_bytes : (size_t)100 << 30;
+    cudaDeviceGetAttribute(&h->sms, cudaDevAttrMultiProcessorCount, device);
+    // keep freed batch memory cached in the stream-ordered pool
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+        uint64_t thr = h->budget;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    }
+    e = cudaStreamCreateWithFlags(&h->sync_stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) { delete h; return set_cuda_error("stream creation", e); }
+    int status = PLP_OK;
+    if (!device_mt_init(&status)) { cudaStreamDestroy(h->sync_stream); delete h; return status; }
+    h->streams.resize(h->n_workers);
+    for (int i = 0; i < h->n_workers; i++) {
+        e = cudaStreamCreateWithFlags(&h->streams[i], cudaStreamNonBlocking);
+        if (e != cudaSuccess) return set_cuda_error("stream creation", e);
+    }
+    for (int i = 0; i < h->n_workers; i++) h->workers.emplace_back(worker_main, h, i);
+    *out = h;
+    return PLP_OK;
+}
+
+void plp_destroy(plp_handle* h) {
+    if (!h) return;
+    {
+        std::lock_guard<std::mutex> lk(h->mu);
+        h->stop = true;
+    }
+    h->cv_sched.notify_all();
+    for (auto& t : h->workers) t.join();
+    for (auto& kv : h->reqs) delete kv.second->result;
+    for (auto s : h->streams) cudaStreamDestroy(s);
+    if (h->sync_stream) cudaStreamDestroy(h->sync_stream);
+    delete h;
+}
+
+int plp_set_tile(plp_handle* h, int32_t P, int32_t C, int32_t D) {
+    if (!h) return set_error(PLP_E_INVALID, "plp_set_tile: null handle");
+    if (P < 0 || C < 0 || D < 0 || D > 8 || P > P_MAX || C > C_MAX) {
+        int s = set_error(PLP_E_INVALID, "plp_set_tile: out of range");
+        record(h, s);
+        return s;
+    }
+    std::lock_guard<std::mutex> g(h->sync_mu);
+    std::lock_guard<std::mutex> lk(h->mu);
+    TileConfig t = h->tile;
+    if (P) t.P = P;
+    if (C) t.C = C;
+    if (D) t.D = D;
+    if (decoder_smem_bytes(t.P, t.C) * t.D > 227 * 1024) {
+        int s = set_error(PLP_E_CAPACITY, "plp_set_tile: tile exceeds shared memory");
+        record(h, s);
+        return s;
+    }
+    h->tile = t;
+    return PLP_OK;
+}
+
+int plp_solve(plp_handle* h, const plp_instance* const* insts, int32_t n_inst,
+              const plp_run_opts* opts, int32_t n_opts, plp_result** results) {
+    if (!h || !insts || !opts || !results || n_inst < 1 || (n_opts != 1 && n_opts != n_inst)) {
+        int s = set_error(PLP_E_INVALID, "plp_solve: bad argument");
+        record(h, s);
+        return s;
+    }
+    std::lock_guard<std::mutex> g(h->sync_mu);
+    cudaSetDevice(h->device);
+    std::vector<const Instance*> in;
+    std::vector<plp_run_opts> op;
+    for (int i = 0; i < n_inst; i++) {
+        if (!insts[i]) {
+            int s = set_error(PLP_E_INVALID, "plp_solve: null instance");
+            record(h, s);
+            return s;
+        }
+        in.push_back(&insts[i]->inst);
+        op.push_back(opts[n_opts == 1 ? 0 : i]);
+    }
+    const double t0 = now_seconds();
+    Batch b;
+    int s = b.build(in, op);
+    TileConfig tile;
+    {
+        std::lock_guard<std::mutex> lk(h->mu);
+        tile = h->tile;
+    }
+    if (s == PLP_OK) s = run_batch(b, h->sync_stream, h->sync_pin, h->sms, tile);
+    if (s == PLP_OK) {
+        std::lock_guard<std::mutex> lk(h->mu);
+        remember_tile(h->tile, tile);
+    }
+    if (s != PLP_OK) {
+        record(h, s);
+        return s;
+    }
+    auto res = collect(b, now_seconds() - t0);
+    for (int i = 0; i < n_inst; i++) results[i] = res[i];
+    return PLP_OK;
+}
+
+int plp_submit(plp_handle* h, const plp_instance* inst, const plp_run_opts* opts, int64_t* id) {
+    if (!h || !inst || !opts || !id) {
+        int s = set_error(PLP_E_INVALID, "plp_submit: null argument");
+        record(h, s);
+        return s;
+    }
+    if (opts->restarts < 1 || opts->passes < 1 || (opts->order != 0 && opts->order != 1)) {
+        int s = set_error(PLP_E_INVALID, "plp_submit: bad options");
+        record(h, s);
+        return s;
+    }
+    auto r = std::make_unique<Request>();
+    r->inst = inst->inst;
+    r->opts = *opts;
+    r->bytes = request_bytes(r->inst, r->opts);
+    if (r->bytes > h->budget) {
+        int s = set_error(PLP_E_BUDGET, "request needs " + std::to_string(r->bytes) +
+                                            " device bytes, more than the handle's budget");
+        record(h, s);
+        return s;
+    }
+    r->t_submit = now_seconds();
+    {
+        std::lock_guard<std::mutex> lk(h->mu);
+        r->id = h->next_id++;
+        *id = r->id;
+        h->queue.push_back(r->id);
+        h->reqs[r->id] = std::move(r);
+    }
+    h->cv_sched.notify_one();
+    return PLP_OK;
+}
+
+int plp_poll(plp_handle* h, int64_t id) {
+    if (!h) return set_error(PLP_E_INVALID, "plp_poll: null handle");
+    std::lock_guard<std::mutex> lk(h->mu);
+    auto it = h->reqs.find(id);
+    if (it == h->reqs.end()) {
+        int s = set_error(PLP_E_NOT_FOUND, "unknown request id");
+        h->err = g_err;
+        return s;
+    }
+    if (it->second->status != PLP_OK && it->second->status != PLP_E_PENDING) {
+        g_err = it->second->err;
+        h->err = g_err;
+    }
+    return it->second->status;
+}
+
+int plp_wait(plp_handle* h, int64_t id, int64_t timeout_ms) {
+    if (!h) return set_error(PLP_E_INVALID, "plp_wait: null handle");
+    std::unique_lock<std::mutex> lk(h->mu);
+    auto it = h->reqs.find(id);
+    if (it == h->reqs.end()) {
+        int s = set_error(PLP_E_NOT_FOUND, "unknown request id");
+        h->err = g_err;
+        return s;
+    }
+    Request* r = it->second.get();
+    auto done = [&] { return r->status != PLP_E_PENDING; };
+    if (timeout_ms < 0) h->cv.wait(lk, done);
+    else if (!h->cv.wait_for(lk, std::chrono::milliseconds(timeout_ms), done)) {
+        int s = set_error(PLP_E_TIMEOUT, "request still running");
+        h->err = g_err;
+        return s;
+    }
+    if (r->status != PLP_OK) {
+        g_err = r->err.empty() ? "request failed" : r->err;
+        h->err = g_err;
+    }
+    return r->status;
+}
+
+int plp_take_result(plp_handle* h, int64_t id, plp_result** out) {
+    if (!h || !out) return set_error(PLP_E_INVALID, "plp_take_result: null argument");
+    std::lock_guard<std::mutex> lk(h->mu);
+    auto it = h->reqs.find(id);
+    if (it == h->reqs.end()) return set_error(PLP_E_NOT_FOUND, "unknown request id");
+    Request* r = it->second.get();
+    if (r->status == PLP_E_PENDING) return set_error(PLP_E_PENDING, "request not finished");
+    const int s = r->status;
+    if (s != PLP_OK) {
+        g_err = r->err.empty() ? "request failed" : r->err;
+        h->reqs.erase(it);
+        return s;
+    }
+    *out = r->result;
+    r->result = nullptr;
+    h->reqs.erase(it);
+    return PLP_OK;
+}
+
+int plp_cancel(plp_handle* h, int64_t id) {
+    if (!h) return set_error(PLP_E_INVALID, "plp_cancel: null handle");
+    {
+        std::lock_guard<std::mutex> lk(h->mu);
+        auto it = h->reqs.find(id);
+        if (it == h->reqs.end()) return set_error(PLP_E_NOT_FOUND, "unknown request id");
+        Request* r = it->second.get();
+        if (r->status != PLP_E_PENDING) return PLP_OK;   // already finished
+        r->cancelled = true;
+        if (!r->running) {
+            r->status = PLP_E_CANCELLED;
+            r->err = "request was cancelled";
+            r->t_done = now_seconds();
+        }
+    }
+    h->cv.notify_all();
+    h->cv_sched.notify_all();
+    return PLP_OK;
+}
+
+int plp_request_times(plp_handle* h, int64_t id, double* queued_s, double* total_s) {
+    if (!h) return set_error(PLP_E_INVALID, "plp_request_times: null handle");
+    std::lock_guard<std::mutex> lk(h->mu);
+    auto it = h->reqs.find(id);
+    if (it == h->reqs.end()) return set_error(PLP_E_NOT_FOUND, "unknown request id");
+    const Request* r = it->second.get();
+    if (queued_s) *queued_s = r->t_start > 0 ? r->t_start - r->t_submit : -1.0;
+    if (total_s) *total_s = r->t_done > 0 ? r->t_done - r->t_submit : -1.0;
+    return PLP_OK;
+}
+
+// ---- prepared batches ------------------------------------------------------
+}  // extern "C"
+
+struct plp_batch {
+    plp_handle* h = nullptr;
+    Batch b;
+    bool executed = false;
+};
+
+extern "C" {
+
+int plp_batch_prepare(plp_handle* h, const plp_instance* const* insts, int32_t n_inst,
+                      const plp_run_opts* opts, int32_t n_opts, plp_batch** out) {
+    if (!h || !insts || !opts || !out || n_inst < 1 || (n_opts != 1 && n_opts != n_inst)) {
+        int s = set_error(PLP_E_INVALID, "plp_batch_prepare: bad argument");
+        record(h, s);
+        return s;
+    }
+    std::lock_guard<std::mutex> g(h->sync_mu);
+    cudaSetDevice(h->device);
+    auto pb = std::make_unique<plp_batch>();
+    pb->h = h;
+    std::vector<const Instance*> in;
+    std::vector<plp_run_opts> op;
+    for (int i = 0; i < n_inst; i++) {
+        if (!insts[i]) {
+            int s = set_error(PLP_E_INVALID, "plp_batch_prepare: null instance");
+            record(h, s);
+            return s;
+        }
+        in.push_back(&insts[i]->inst);
+        op.push_back(opts[n_opts == 1 ? 0 : i]);
+    }
+    int s = pb->b.build(in, op);
+    TileConfig tile;
+    {
+        std::lock_guard<std::mutex> lk(h->mu);
+        tile = h->tile;
+    }
+    if (s == PLP_OK) s = batch_prepare(pb->b, h->sync_stream, h->sync_pin, h->sms, tile);
+    if (s != PLP_OK) {
+        record(h, s);
+        return s;
+    }
+    *out = pb.release();
+    return PLP_OK;
+}
+
+int plp_batch_run(plp_batch* pb, double* device_ms, double* decoder_ms, int32_t* launches) {
+    if (!pb) return set_error(PLP_E_INVALID, "plp_batch_run: null batch");
+    plp_handle* h = pb->h;
+    std::lock_guard<std::mutex> g(h->sync_mu);
+    cudaSetDevice(h->device);
+    TileConfig tile;
+    {
+        std::lock_guard<std::mutex> lk(h->mu);
+        tile = h->tile;
+    }
+    ExecStats x;
+    int s = batch_execute(pb->b, h->sync_stream, h->sms, tile, &x);
+    if (s != PLP_OK) {
+        record(h, s);
+        return s;
+    }
+    {
+        std::lock_guard<std::mutex> lk(h->mu);
+        remember_tile(h->tile, tile);
+    }
+    pb->executed = true;
+    if (device_ms) *device_ms = x.device_ms;
+    if (decoder_ms) *decoder_ms = x.decoder_ms;
+    if (launches) *launches = x.launches;
+    return PLP_OK;
+}
+
+int plp_batch_fetch(plp_batch* pb, plp_result** results) {
+    if (!pb || !results) return set_error(PLP_E_INVALID, "plp_batch_fetch: null argument");
+    if (!pb->executed) return set_error(PLP_E_INVALID, "plp_batch_fetch: batch has not run");
+    plp_handle* h = pb->h;
+    std::lock_guard<std::mutex> g(h->sync_mu);
+    cudaSetDevice(h->device);
+    const double t0 = now_seconds();
+    int s = batch_fetch(pb->b, h->sync_stream);
+    if (s != PLP_OK) {
+        record(h, s);
+        return s;
+    }
+    auto res = collect(pb->b, now_seconds() - t0);
+    for (size_t i = 0; i < res.size(); i++) results[i] = res[i];
+    return PLP_OK;
+}
+
+int plp_batch_io_bytes(const plp_batch* pb, int64_t* h2d, int64_t* d2h) {
+    if (!pb) return set_error(PLP_E_INVALID, "plp_batch_io_bytes: null batch");
+    if (h2d) *h2d = (int64_t)batch_h2d_bytes(pb->b);
+    if (d2h) *d2h = (int64_t)batch_d2h_bytes(pb->b);
+    return PLP_OK;
+}
+
+void plp_batch_free(plp_batch* pb) {
+    if (!pb) return;
+    {
+        std::lock_guard<std::mutex> g(pb->h->sync_mu);
+        batch_release(pb->b, pb->h->sync_stream);
+    }
+    delete pb;
+}
+
+// ---- reference work accounting ---------------------------------------------
+int plp_result_work(const plp_result* r, int32_t k, int64_t* aabb_tests, int64_t* pairs) {
+    if (!r) return set_error(PLP_E_INVALID, "plp_result_work: null result");
+    if (k < 0 || k >= r->restarts) return set_error(PLP_E_INVALID, "restart out of range");
+    std::vector<Placement> pl;
+    int s = expand(r, k, pl);
+    if (s != PLP_OK) return s;
+    // Replays the reference candidate list (origin + corners of placed boxes,
+    // minus points strictly inside one) step by step. The step at which each
+    // box was placed is recovered greedily: a step whose type differs from the
+    // next placed box was skipped; a skipped step of type t leaves the state
+    // unchanged, so the next step of type t would fail too -- hence the next
+    // box of type t is always placed at the first step of type t that comes.
+    std::vector<std::array<int, 3>> cand{{0, 0, 0}};   // (z, y, x), sorted, unique
+    long long T = 0, Pn = 0;
+    size_t idx = 0;
+    for (int t : r->steps) {
+        const TypeOrs& o = r->ors[t];
+        if (o.n == 0) continue;
+        long long c2 = 0;
+        for (const auto& p : cand)
+            for (int q = 0; q < o.n; q++)
+                c2 += (p[2] + o.w[q] <= r->L && p[1] + o.d[q] <= r->W && p[0] + o.h[q] <= r->H);
+        T += 2LL * (long long)idx * c2;
+        Pn += (long long)cand.size() * o.n;
+        if (idx < pl.size() && pl[idx].type == t) {
+            const Placement& b = pl[idx++];
+            std::vector<std::array<int, 3>> nc;
+            nc.reserve(cand.size() + 8);
+            for (const auto& p : cand)
+                if (!(b.x < p[2] && p[2] < b.x + b.w && b.y < p[1] && p[1] < b.y + b.d && b.z < p[0] &&
+                      p[0] < b.z + b.h))
+                    nc.push_back(p);
+            for (int c = 0; c < 8; c++)
+                nc.push_back({b.z + ((c & 4) ? b.h : 0), b.y + ((c & 2) ? b.d : 0), b.x + ((c & 1) ? b.w : 0)});
+            std::sort(nc.begin(), nc.end());
+            nc.erase(std::unique(nc.begin(), nc.end()), nc.end());
+            cand.swap(nc);
+        }
+    }
+    if (aabb_tests) *aabb_tests = T;
+    if (pairs) *pairs = Pn;
+    return PLP_OK;
+}
+
+// ---- kernel hooks -----------------------------------------------------------
+int plp_rng_dump(const int64_t* seeds, int32_t n_seeds, int32_t n_random, int32_t n_bits,
+                 int32_t k_bits, double* out_random, uint32_t* out_bits) {
+    if (!seeds || n_seeds < 0 || n_random < 0 || n_bits < 0 || k_bits < 1 || k_bits > 32 ||
+        (n_random && !out_random) || (n_bits && !out_bits))
+        return set_error(PLP_E_INVALID, "plp_rng_dump: bad argument");
+    if (n_seeds == 0) return PLP_OK;
+    int status = PLP_OK;
+    const uint32_t* mt_init = device_mt_init(&status);
+    if (!mt_init) return status;
+    const size_t sb = (size_t)n_seeds * 8, rb = (size_t)n_seeds * n_random * 8,
+                 bb = (size_t)n_seeds * n_bits * 4;
+    char* d = nullptr;
+    cudaError_t e = cudaMalloc(&d, sb + rb + bb + 64);
+    if (e != cudaSuccess) return set_cuda_error("plp_rng_dump: allocation", e);
+    e = cudaMemcpy(d, seeds, sb, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = launch_rng_dump(reinterpret_cast<const long long*>(d), n_seeds, n_random, n_bits, k_bits,
+                            mt_init, reinterpret_cast<double*>(d + sb),
+                            reinterpret_cast<uint32_t*>(d + sb + rb), nullptr);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e == cudaSuccess && rb) e = cudaMemcpy(out_random, d + sb, rb, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && bb) e = cudaMemcpy(out_bits, d + sb + rb, bb, cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) return set_cuda_error("plp_rng_dump", e);
+    return PLP_OK;
+}
+
+int plp_rng_dump_host(const int64_t* seeds, int32_t n_seeds, int32_t n_random, int32_t n_bits,
+                      int32_t k_bits, double* out_random, uint32_t* out_bits) {
+    if (!seeds || n_seeds < 0 || n_random < 0 || n_bits < 0 || k_bits < 1 || k_bits > 32 ||
+        (n_random && !out_random) || (n_bits && !out_bits))
+        return set_error(PLP_E_INVALID, "plp_rng_dump_host: bad argument");
+    for (int s = 0; s < n_seeds; s++) {
+        const int64_t v = seeds[s];
+        PyRng rng((uint64_t)(v < 0 ? -v : v));
+        for (int i = 0; i < n_random; i++) out_random[(size_t)s * n_random + i] = rng.random();
+        for (int i = 0; i < n_bits; i++) out_bits[(size_t)s * n_bits + i] = rng.getrandbits(k_bits);
+    }
+    return PLP_OK;
+}
+
+int plp_fsr_score(const int32_t* rows7, const int32_t* offsets, int32_t n_pack, double mu,
+                  double* out_score, double* out_fsr) {
+    if (!offsets || n_pack < 0 || !out_score) return set_error(PLP_E_INVALID, "plp_fsr_score: bad argument");
+    if (n_pack == 0) return PLP_OK;
+    const int total = offsets[n_pack];
+    int cap = 32;
+    for (int i = 0; i < n_pack; i++) {
+        const int n = offsets[i + 1] - offsets[i];
+        if (n < 0) return set_error(PLP_E_INVALID, "plp_fsr_score: offsets must be nondecreasing");
+        while (cap < n) cap += 32;
+    }
+    if (total && !rows7) return set_error(PLP_E_INVALID, "plp_fsr_score: null rows");
+    if (fsr_smem_per_warp(cap) * 4 > 227 * 1024)
+        return set_error(PLP_E_CAPACITY, "plp_fsr_score: packing larger than the shared-memory tile");
+    const size_t rb = (size_t)total * 28, ob = (size_t)(n_pack + 1) * 4, scb = (size_t)n_pack * 8,
+                 fb = (size_t)total * 8;
+    const size_t o_off = (rb + 255) & ~size_t(255), o_sc = o_off + ((ob + 255) & ~size_t(255)),
+                 o_f = o_sc + ((scb + 255) & ~size_t(255));
+    char* d = nullptr;
+    cudaError_t e = cudaMalloc(&d, o_f + fb + 64);
+    if (e != cudaSuccess) return set_cuda_error("plp_fsr_score: allocation", e);
+    if (rb) e = cudaMemcpy(d, rows7, rb, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(d + o_off, offsets, ob, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = launch_fsr(reinterpret_cast<const int*>(d), reinterpret_cast<const int*>(d + o_off), n_pack,
+                       cap, mu, reinterpret_cast<double*>(d + o_sc),
+                       out_fsr ? reinterpret_cast<double*>(d + o_f) : nullptr, nullptr);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = cudaMemcpy(out_score, d + o_sc, scb, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && out_fsr && fb) e = cudaMemcpy(out_fsr, d + o_f, fb, cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) return set_cuda_error("plp_fsr_score", e);
+    return PLP_OK;
+}
+
+int plp_item_order(const plp_instance* const* insts, int32_t n_inst, int32_t order,
+                   int32_t* out_types, int64_t* out_offsets) {
+    if (!insts || n_inst < 0 || !out_offsets || (order != 0 && order != 1))
+        return set_error(PLP_E_INVALID, "plp_item_order: bad argument");
+    std::vector<long long> vols;
+    std::vector<int> qty, toff, nt;
+    std::vector<long long> soff{0};
+    int maxn = 1;
+    for (int i = 0; i < n_inst; i++) {
+        const Instance& I = insts[i]->inst;
+        if (I.types.size() >= 65536) return set_error(PLP_E_CAPACITY, "plp_item_order: too many types");
+        toff.push_back((int)vols.size());
+        nt.push_back((int)I.types.size());
+        for (const auto& t : I.types) {
+            if (t.volume() >= 0x7fffffffLL || t.qty >= 65536)
+                return set_error(PLP_E_CAPACITY, "plp_item_order: volume or quantity beyond the sort key");
+            vols.push_back(t.volume());
+            qty.push_back(t.qty);
+        }
+        soff.push_back(soff.back() + I.n_items());
+        maxn = std::max(maxn, I.n_items());
+    }
+    int cap = 1;
+    while (cap < maxn) cap <<= 1;
+    if (8 * cap > 227 * 1024) return set_error(PLP_E_CAPACITY, "plp_item_order: instance too large");
+    for (int i = 0; i <= n_inst; i++) out_offsets[i] = soff[i];
+    if (n_inst == 0 || soff.back() == 0) return PLP_OK;
+    if (!out_types) return set_error(PLP_E_INVALID, "plp_item_order: null output");
+    const size_t vb = vols.size() * 8 + 8, qb = qty.size() * 4 + 4, tb = (size_t)n_inst * 4,
+                 ob = soff.size() * 8, outb = (size_t)soff.back() * 4;
+    size_t o = 0;
+    auto take = [&](size_t n) { size_t r = o; o += (n + 255) & ~size_t(255); return r; };
+    const size_t o_v = take(vb), o_q = take(qb), o_t = take(tb), o_n = take(tb), o_s = take(ob),
+                 o_out = take(outb);
+    char* d = nullptr;
+    cudaError_t e = cudaMalloc(&d, o);
+    if (e != cudaSuccess) return set_cuda_error("plp_item_order: allocation", e);
+    if (!vols.empty()) e = cudaMemcpy(d + o_v, vols.data(), vols.size() * 8, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && !qty.empty()) e = cudaMemcpy(d + o_q, qty.data(), qty.size() * 4, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(d + o_t, toff.data(), tb, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(d + o_n, nt.data(), tb, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(d + o_s, soff.data(), ob, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = launch_item_order(reinterpret_cast<const long long*>(d + o_v),
+                              reinterpret_cast<const int*>(d + o_q), reinterpret_cast<const int*>(d + o_t),
+                              reinterpret_cast<const int*>(d + o_n),
+                              reinterpret_cast<const long long*>(d + o_s), n_inst, order,
+                              reinterpret_cast<int*>(d + o_out), cap, nullptr);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = cudaMemcpy(out_types, d + o_out, outb, cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) return set_cuda_error("plp_item_order", e);
+    return PLP_OK;
+}
+
+// ---- formatting -------------------------------------------------------------
+int plp_py_repr(double x, char* buf, size_t cap) {
+    if (!buf || !cap) return set_error(PLP_E_INVALID, "plp_py_repr: null buffer");
+    const std::string s = py_repr(x);
+    if (s.size() + 1 > cap) return set_error(PLP_E_INVALID, "plp_py_repr: buffer too small");
+    std::memcpy(buf, s.c_str(), s.size() + 1);
+    return PLP_OK;
+}
+
+int plp_selftest(char* buf, size_t cap, size_t* needed) {
+    std::string o;
+    char line[64];
+    for (unsigned s : {0u, 1u, 7u, 123456789u}) {
+        PyRng rng(s);
+        o += "SEED " + std::to_string(s) + "\n";
+        for (int i = 0; i < 16; i++) {
+            const double v = rng.random();
+            unsigned long long bits;
+            std::memcpy(&bits, &v, 8);
+            std::snprintf(line, sizeof line, "%016llx\n", bits);
+            o += line;
+        }
+        for (int i = 0; i < 16; i++) o += std::to_string(rng.getrandbits(13)) + "\n";
+    }
+    const double vals[] = {0.0, 1.0, 0.5, 0.1, 2.0 / 3.0, 0.5785123966942148,
+                           0.6132075471698113, 0.6595744680851063, 1e-05, 1e-04,
+                           1e15, 1e16, 0.001, 123456789.5, 1.0 / 121.0, 1.0 / 106.0};
+    for (double v : vals) o += "REPR " + py_repr(v) + "\n";
+    if (needed) *needed = o.size();
+    if (buf && cap) {
+        const size_t n = std::min(cap - 1, o.size());
+        std::memcpy(buf, o.data(), n);
+        buf[n] = '\0';
+    }
+    return PLP_OK;
+}
+
+}  // extern "C"
+
+// ---- plain-path scorer -----------------------------------------------------
+namespace plpb {
+
+int device_fsr_score(const std::vector<Placement>& p, double mu, double* score) {
+    std::vector<int32_t> rows;
+    rows.reserve(p.size() * 7);
+    for (const auto& q : p) rows.insert(rows.end(), {q.type, q.x, q.y, q.z, q.w, q.d, q.h});
+    const int32_t off[2] = {0, (int32_t)p.size()};
+    return plp_fsr_score(rows.data(), off, 1, mu, score, nullptr);
+}
+
+}  // namespace plpb

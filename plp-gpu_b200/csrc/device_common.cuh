@@ -1,0 +1,181 @@
+// device_common.cuh -- tables shared by host and device, and device helpers
+// (CPython-exact MT19937 with a warp-cooperative twist, point keys).
+//
+// All device code is compiled with --fmad=false so no double expression is
+// contracted; every FP64 expression keeps the reference operand order.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace plpb {
+
+constexpr unsigned FULL = 0xffffffffu;
+
+// One instance of a batched solve (device copy). Points (x, y, z) are packed
+// into 32-bit keys z << (xb + yb) | y << xb | x, whose numeric order is the
+// reference candidate order (z, y, x) (gpu/plp_common.hpp:282-291).
+struct InstDesc {
+    int L, W, H;
+    int n_steps;         // decode steps (items in sequence order)
+    int step_off;        // first entry in the step-type table
+    int type_off;        // first entry in the orientation table
+    int xb, yb;          // key field widths (bit length of L and W)
+    int restarts;
+    int slot_base;       // result slot of restart 0
+    int place_stride;    // placement capacity per slot (= n_steps)
+    int passes;
+    long long place_off; // first placement of restart 0
+    long long seed;      // restart k is seeded with |seed + k|
+    double eps, theta, mu;
+    int has_theta, first_fit;
+};
+
+// Orientation table entry of one box type: up to 6 (w, d, h), dedup'd in the
+// reference's parser order (gpu/plp_common.hpp:269-280); unused slots are 0.
+struct TypeOrs {
+    int n;
+    int w[6], d[6], h[6];
+    int pad[3];
+};
+static_assert(sizeof(TypeOrs) == 88, "TypeOrs layout");
+
+// Per-restart result head. The placements of the selected pass follow in the
+// placement table, one packed 64-bit word each (see pack_place).
+struct SlotHead {
+    int n_boxes;
+    int err;             // 0 or a DecodeErr value
+    long long volume;
+    double score;
+    int n_passes;
+    int fallback;        // 1: no pass reached theta (reference D4' flag)
+};
+static_assert(sizeof(SlotHead) == 32, "SlotHead layout");
+
+enum DecodeErr : int {
+    ERR_NONE = 0,
+    ERR_BOX_CAP = 1,     // more placed boxes than the shared-memory tile holds
+    ERR_CAND_CAP = 2,    // more live extreme points than the tile holds
+    ERR_RNG = 3,         // randrange rejection loop exceeded its bound
+};
+
+// placement word: x | y << 16 | z << 32 | orientation << 48 | type << 51
+__host__ __device__ inline unsigned long long pack_place(int x, int y, int z, int oi, int type) {
+    return (unsigned long long)(unsigned)x | ((unsigned long long)(unsigned)y << 16) |
+           ((unsigned long long)(unsigned)z << 32) | ((unsigned long long)(unsigned)oi << 48) |
+           ((unsigned long long)(unsigned)type << 51);
+}
+__host__ __device__ inline void unpack_place(unsigned long long v, int& x, int& y, int& z,
+                                             int& oi, int& type) {
+    x = (int)(v & 0xffff);
+    y = (int)((v >> 16) & 0xffff);
+    z = (int)((v >> 32) & 0xffff);
+    oi = (int)((v >> 48) & 7);
+    type = (int)(v >> 51);
+}
+
+#ifdef __CUDACC__
+
+__device__ __forceinline__ unsigned lanemask_lt() {
+    unsigned m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+// ---------------------------------------------------------------------------
+// MT19937 (Matsumoto & Nishimura), CPython seeding and draws.
+// State lives in shared memory, the read position in a warp-uniform register;
+// every lane of the warp calls the draw functions with identical arguments.
+// ---------------------------------------------------------------------------
+
+// init_by_array on |seed| (one or two 32-bit key words), starting from the
+// seed-independent init_genrand(19650218) table `init`. The recurrence is
+// serial: lane 0 runs it, the warp then syncs.
+__device__ inline void mt_seed_warp(uint32_t* mt, unsigned long long seed_abs,
+                                    const uint32_t* __restrict__ init, int lane) {
+    for (int i = lane; i < 624; i += 32) mt[i] = init[i];
+    __syncwarp();
+    if (lane == 0) {
+        const uint32_t k0 = (uint32_t)seed_abs;
+        const uint32_t k1 = (uint32_t)(seed_abs >> 32);
+        const int nkey = k1 ? 2 : 1;
+        uint32_t prev = mt[0];
+        int i = 1, j = 0;
+        for (int k = 624; k > 0; k--) {
+            const uint32_t t = prev ^ (prev >> 30);
+            const uint32_t v = (mt[i] ^ (t * 1664525u)) + (j ? k1 : k0) + (uint32_t)j;
+            mt[i] = v;
+            prev = v;
+            if (++i >= 624) { mt[0] = v; i = 1; }
+            if (++j >= nkey) j = 0;
+        }
+        for (int k = 623; k > 0; k--) {
+            const uint32_t t = prev ^ (prev >> 30);
+            const uint32_t v = (mt[i] ^ (t * 1566083941u)) - (uint32_t)i;
+            mt[i] = v;
+            prev = v;
+            if (++i >= 624) { mt[0] = v; i = 1; }
+        }
+        mt[0] = 0x80000000u;
+    }
+    __syncwarp();
+}
+
+// Regenerates all 624 words. Word i needs old words i, i+1 and word
+// (i + 397) mod 624, which is still old for i < 227 and already new for
+// i >= 227. Chunks of 32 in increasing i therefore only read finished or
+// untouched words; inside a chunk all lanes read before any lane writes.
+__device__ inline void mt_twist_warp(uint32_t* mt, int lane) {
+    for (int base = 0; base < 623; base += 32) {
+        const int i = base + lane;
+        uint32_t nv = 0;
+        if (i < 623) {
+            const uint32_t y = (mt[i] & 0x80000000u) | (mt[i + 1] & 0x7fffffffu);
+            const int k = i < 227 ? i + 397 : i - 227;
+            nv = mt[k] ^ (y >> 1) ^ ((y & 1u) ? 0x9908b0dfu : 0u);
+        }
+        __syncwarp();
+        if (i < 623) mt[i] = nv;
+        __syncwarp();
+    }
+    if (lane == 0) {
+        const uint32_t y = (mt[623] & 0x80000000u) | (mt[0] & 0x7fffffffu);
+        mt[623] = mt[396] ^ (y >> 1) ^ ((y & 1u) ? 0x9908b0dfu : 0u);
+    }
+    __syncwarp();
+}
+
+__device__ __forceinline__ uint32_t mt_next(uint32_t* mt, int& pos, int lane) {
+    if (pos >= 624) {
+        mt_twist_warp(mt, lane);
+        pos = 0;
+    }
+    uint32_t y = mt[pos++];
+    y ^= y >> 11;
+    y ^= (y << 7) & 0x9d2c5680u;
+    y ^= (y << 15) & 0xefc60000u;
+    y ^= y >> 18;
+    return y;
+}
+
+// CPython random(): (a * 2^26 + b) / 2^53 with a = 27 bits, b = 26 bits.
+__device__ __forceinline__ double mt_random(uint32_t* mt, int& pos, int lane) {
+    const uint32_t a = mt_next(mt, pos, lane) >> 5;
+    const uint32_t b = mt_next(mt, pos, lane) >> 6;
+    return ((double)a * 67108864.0 + (double)b) * (1.0 / 9007199254740992.0);
+}
+
+// CPython randrange(n), n >= 1: getrandbits(bit_length(n)) until < n.
+// Returns -1 if the (astronomically unlikely) rejection bound is hit.
+__device__ __forceinline__ int mt_randrange(uint32_t* mt, int& pos, int lane, int n) {
+    const int k = 32 - __clz(n);
+    for (int tries = 0; tries < 4096; tries++) {
+        const uint32_t r = mt_next(mt, pos, lane) >> (32 - k);
+        if (r < (uint32_t)n) return (int)r;
+    }
+    return -1;
+}
+
+#endif  // __CUDACC__
+
+}  // namespace plpb

@@ -1,0 +1,47 @@
+// engine.hpp -- host-side launchers of the device kernels (internal).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "device_common.cuh"
+
+namespace plpb {
+
+struct DecodeLaunch {
+    const InstDesc* inst;
+    const int* step_type;
+    const TypeOrs* types;
+    const int2* work;
+    int n_work;
+    int* work_next;
+    int* err_flag;            // OR of (1 << err) over restarts that failed
+    SlotHead* heads;
+    unsigned long long* places;
+    unsigned long long* scratch;
+    const uint32_t* mt_init;
+    int P, C;                 // shared-memory tile: boxes and live points per decoder
+    int decoders_per_cta;     // warps (decoders) per CTA, <= 8
+    int ctas;
+};
+
+int decoder_smem_bytes(int P, int C);
+cudaError_t decoder_occupancy(int P, int C, int decoders_per_cta, int* ctas_per_sm);
+cudaError_t launch_decoder(const DecodeLaunch& L, cudaStream_t st);
+cudaError_t launch_select_best(const InstDesc* inst, int n_inst, const SlotHead* heads, int2* best,
+                               cudaStream_t st);
+cudaError_t launch_rng_dump(const long long* seeds, int n_seeds, int n_random, int n_bits,
+                            int k_bits, const uint32_t* mt_init, double* out_r, uint32_t* out_b,
+                            cudaStream_t st);
+int fsr_smem_per_warp(int cap);
+cudaError_t launch_fsr(const int* rows7, const int* offsets, int n_pack, int cap, double mu,
+                       double* out_score, double* out_fsr, cudaStream_t st);
+cudaError_t launch_item_order(const long long* vols, const int* qty, const int* type_off,
+                              const int* n_types, const long long* step_off, int n_inst, int order,
+                              int* out_types, int sort_cap, cudaStream_t st);
+// one-step feasibility (kernel a); first_out (optional) receives the smallest
+// feasible pair index (atomicMin; caller initialises it to INT_MAX)
+cudaError_t launch_feas(const int* cand, int n_cand, const int* ors, int n_ors, const int* fast6,
+                        int n_fast, int L, int W, int H, unsigned char* bits, int* first_out,
+                        cudaStream_t st);
+
+}  // namespace plpb

@@ -1,0 +1,178 @@
+#!/usr/bin/env python3
+"""Regenerates the golden fixtures in tests/golden/ (run in a container that
+has the reference tree at /root/reference and the reference programs built
+with `make -C oracle ref`).
+
+Fixtures:
+  selftest_ref.txt   the reference --selftest protocol (4 seeds x 16 random()
+                     bit patterns + 16 getrandbits(13), then 16 repr lines),
+                     produced by CPython's own random and repr
+  rng_vectors.json   CPython random.Random(seed) streams for small, 2-word
+                     (>= 2**32) and negative seeds: random(), getrandbits(k),
+                     randrange(n)
+  repr_vectors.json  CPython repr() of doubles (random bit patterns, c/n ratios)
+  decoder.jsonl      per-restart JSON of the reference's g++ build
+                     (gpu/plp_common.hpp via oracle/_ref/ref_harness) on the
+                     seeded synthetic workloads, time_s removed; every case also
+                     cross-checked here against the reference CPython solver
+                     (plp.solver.run) on a sample of restarts
+"""
+from __future__ import annotations
+
+import hashlib
+import json
+import os
+import random
+import struct
+import subprocess
+import sys
+import tempfile
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.join(REPO, "plp-gpu_b200"))
+from plpb200 import synth  # noqa: E402
+
+REF = "/root/reference"
+HARNESS = os.path.join(REPO, "oracle", "_ref", "ref_harness")
+
+
+def bits_of(x: float) -> str:
+    return format(struct.unpack("<Q", struct.pack("<d", x))[0], "016x")
+
+
+def make_selftest() -> str:
+    out = []
+    for s in (0, 1, 7, 123456789):
+        out.append(f"SEED {s}")
+        r = random.Random(s)
+        out += [bits_of(r.random()) for _ in range(16)]
+        out += [str(r.getrandbits(13)) for _ in range(16)]
+    vals = (0.0, 1.0, 0.5, 0.1, 2.0 / 3.0, 0.5785123966942148, 0.6132075471698113,
+            0.6595744680851063, 1e-05, 1e-04, 1e15, 1e16, 0.001, 123456789.5, 1.0 / 121.0, 1.0 / 106.0)
+    out += [f"REPR {repr(v)}" for v in vals]
+    return "\n".join(out) + "\n"
+
+
+def make_rng_vectors() -> dict:
+    seeds = [0, 1, 2, 7, 1023, 123456789, 2**31 - 1, 2**32 - 1, 2**32, 2**32 + 5, 2**40 + 12345,
+             2**63 - 1, -1, -7, -(2**33)]
+    out = []
+    for s in seeds:
+        r = random.Random(s)
+        rnd = [bits_of(r.random()) for _ in range(700)]       # crosses a twist
+        gb = {k: [r.getrandbits(k) for _ in range(8)] for k in (1, 5, 13, 31, 32)}
+        rr = {n: [r.randrange(n) for _ in range(16)] for n in (1, 2, 3, 7, 100, 1000, 65537)}
+        out.append({"seed": s, "random_bits": rnd, "getrandbits": gb, "randrange": rr})
+    return {"vectors": out}
+
+
+def make_repr_vectors() -> dict:
+    r = random.Random(99)
+    vals = []
+    for _ in range(2000):
+        b = r.getrandbits(64)
+        x = struct.unpack("<d", struct.pack("<Q", b))[0]
+        if x != x or x in (float("inf"), float("-inf")):
+            continue
+        vals.append(x)
+    for n in range(1, 260):
+        for c in range(0, n + 1, max(1, n // 17)):
+            vals.append(c / n)
+    vals += [1e-5, 1e-4, 1e15, 1e16, 1e17, 123456789.5, 0.1, 1 / 3, 2 / 3, 5e-324, 1.7976931348623157e308]
+    return {"values": [[bits_of(v), repr(v)] for v in vals]}
+
+
+CASES = [
+    # (name, generator, restart seeds, passes, flags)
+    ("single_pass", lambda: [synth.single_pass(1)], [1], 1,
+     ["--eps", "0", "--no-theta", "--order", "volume"]),
+    ("single_pass_theta", lambda: [synth.single_pass(1)], [0, 1, 2], 1, ["--eps", "0.3"]),
+    ("single_pass_input", lambda: [synth.single_pass(1)], [4, 5], 1, ["--order", "input"]),
+    ("single_pass_firstfit", lambda: [synth.single_pass(1)], [3], 1, ["--first-fit"]),
+    ("multi_restart", lambda: [synth.multi_restart(2)], list(range(64)), 1, []),
+    ("multi_restart_passes3", lambda: [synth.multi_restart(2)], list(range(8)), 3, []),
+    ("multi_restart_mu", lambda: [synth.multi_restart(2)], [0, 1], 1, ["--mu", "0.45"]),
+    ("batched", lambda: synth.batched_set(8), [0, 1, 2, 3], 1, []),
+    ("stress", lambda: synth.stress_set(2), [0, 1, 2, 3], 1, []),
+]
+
+
+def harness(path, seeds, passes, flags):
+    assert seeds == list(range(seeds[0], seeds[0] + len(seeds))), "seeds must be contiguous"
+    cmd = [HARNESS, path, "--seed", str(seeds[0]), "--restarts", str(len(seeds)), "--passes",
+           str(passes), "--threads", "8", "--json"] + flags
+    out = subprocess.run(cmd, capture_output=True, text=True, check=True).stdout
+    rows = [json.loads(line) for line in out.splitlines()]
+    for r in rows:
+        r.pop("time_s")
+    return rows
+
+
+def python_ref(inst_text, seed, passes, flags):
+    """Reference CPython solver, fixed pass count (single pass only)."""
+    sys.path.insert(0, REF)
+    from plp.parser import parse
+    from plp.solver import run
+    inst = parse(inst_text)[0]
+    kw = dict(eps=0.3, theta=0.9, order="volume", first_fit=False, single_pass=True)
+    i = 0
+    while i < len(flags):
+        f = flags[i]
+        if f == "--eps":
+            kw["eps"] = float(flags[i + 1]); i += 2
+        elif f == "--no-theta":
+            kw["theta"] = None; i += 1
+        elif f == "--order":
+            kw["order"] = flags[i + 1]; i += 2
+        elif f == "--first-fit":
+            kw["first_fit"] = True; i += 1
+        elif f == "--mu":
+            return None
+        else:
+            raise ValueError(f)
+    if passes != 1:
+        return None
+    r = run(inst, seed=seed, time_limit_s=0, **kw)
+    return {"n_boxes": r.n_boxes, "volume_cm3": r.volume, "stability_score": r.score,
+            "fallback": r.fallback, "n_passes": r.n_passes, "seed": r.seed,
+            "placements": [list(p) for p in r.placements]}
+
+
+def make_decoder() -> list:
+    rows = []
+    with tempfile.TemporaryDirectory() as td:
+        for name, gen, seeds, passes, flags in CASES:
+            for ii, inst in enumerate(gen()):
+                text = inst.to_thpack()
+                path = os.path.join(td, f"{name}_{ii}.txt")
+                with open(path, "w") as f:
+                    f.write(text)
+                got = harness(path, seeds, passes, flags)
+                # cross-check a sample against the reference CPython solver
+                for k in (0, len(seeds) - 1):
+                    py = python_ref(text, seeds[k], passes, flags)
+                    if py is not None and py != got[k]:
+                        raise SystemExit(f"g++ and CPython reference disagree on {name}/{ii}/{seeds[k]}")
+                rows.append({"case": name, "instance": ii, "inst_seed": inst.seed,
+                             "sha256": hashlib.sha256(text.encode()).hexdigest(),
+                             "seeds": seeds, "passes": passes, "flags": flags, "expected": got})
+    return rows
+
+
+def main():
+    with open(os.path.join(HERE, "selftest_ref.txt"), "w") as f:
+        f.write(make_selftest())
+    with open(os.path.join(HERE, "rng_vectors.json"), "w") as f:
+        json.dump(make_rng_vectors(), f, separators=(",", ":"))
+    with open(os.path.join(HERE, "repr_vectors.json"), "w") as f:
+        json.dump(make_repr_vectors(), f, separators=(",", ":"))
+    rows = make_decoder()
+    with open(os.path.join(HERE, "decoder.jsonl"), "w") as f:
+        for r in rows:
+            f.write(json.dumps(r, separators=(",", ":")) + "\n")
+    print("wrote", len(rows), "decoder cases")
+
+
+if __name__ == "__main__":
+    main()

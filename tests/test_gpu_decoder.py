@@ -1,0 +1,108 @@
+"""GPU parity of the persistent decoder (plp_solve) and the plain path
+(plp_run_plain) against the reference g++ goldens and the CPU oracle.
+
+Every restart's JSON (time_s excluded, as parity/compare_parity.py:30-31
+does) must be identical.
+"""
+import json
+import os
+
+import pytest
+
+import oracle_py as O
+import plpb200 as P
+from conftest import GOLDEN
+from plpb200 import synth
+from test_oracle_pins import _golden_cases, _instance_for, flags_to_kw
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def handle():
+    h = P.Handle()
+    yield h
+    h.close()
+
+
+def _opts(seed, restarts, passes, kw, best_only=False):
+    return P.make_opts(seed=seed, restarts=restarts, passes=passes, eps=kw["eps"], theta=kw["theta"],
+                       order=kw["order"], first_fit=kw["first_fit"], mu=kw["mu"], best_only=best_only)
+
+
+@pytest.mark.parametrize("case", _golden_cases(), ids=lambda c: f"{c['case']}-{c['instance']}")
+def test_solve_matches_reference_goldens(handle, case):
+    inst = P.Instance.parse(_instance_for(case))
+    kw = flags_to_kw(case["flags"])
+    res = handle.solve([inst], _opts(case["seeds"][0], len(case["seeds"]), case["passes"], kw))[0]
+    for k, exp in enumerate(case["expected"]):
+        assert O.strip_time(res.json(k)) == exp, (case["case"], k)
+
+
+def test_solve_batched_uneven_matches_oracle(handle):
+    insts = synth.batched_set(24, base_seed=31000) + synth.stress_set(2, base_seed=41000)
+    ps = [P.Instance.parse(i.to_thpack()) for i in insts]
+    res = handle.solve(ps, P.make_opts(seed=100, restarts=3))
+    for i, r in zip(insts, res):
+        oi = O.OInstance(i.to_thpack())
+        for k in range(3):
+            js, _, _ = O.run(oi, seed=100 + k)
+            assert O.strip_time(r.json(k)) == O.strip_time(js)
+
+
+def test_solve_many_restarts_and_best(handle):
+    text = synth.multi_restart(2).to_thpack()
+    inst = P.Instance.parse(text)
+    r = handle.solve([inst], P.make_opts(seed=0, restarts=256))[0]
+    oi = O.OInstance(text)
+    summ = []
+    for k in range(0, 256, 5):
+        js, s, _ = O.run(oi, seed=k)
+        assert O.strip_time(r.json(k)) == O.strip_time(js)
+    for k in range(256):
+        summ.append(r.summary(k))
+    # best: accepted first, then (volume, n_boxes), earliest on ties
+    key = lambda k: (not summ[k].fallback, summ[k].volume, summ[k].n_boxes, -k)
+    best = max(range(256), key=key)
+    assert r.best() == (best, summ[best].fallback)
+
+
+def test_solve_tiny_tile_retries_give_same_results(handle):
+    text = synth.stress(40003).to_thpack()
+    inst = P.Instance.parse(text)
+    h2 = P.Handle()
+    h2.set_tile(16, 32, 4)
+    r_small = h2.solve([inst], P.make_opts(seed=7, restarts=8))[0]
+    h2.close()
+    r_ref = handle.solve([inst], P.make_opts(seed=7, restarts=8))[0]
+    oi = O.OInstance(text)
+    for k in range(8):
+        js, _, _ = O.run(oi, seed=7 + k)
+        assert O.strip_time(r_small.json(k)) == O.strip_time(js) == O.strip_time(r_ref.json(k))
+
+
+def test_solve_best_only(handle):
+    text = synth.batched(30005).to_thpack()
+    inst = P.Instance.parse(text)
+    full = handle.solve([inst], P.make_opts(seed=3, restarts=16))[0]
+    bo = handle.solve([inst], P.make_opts(seed=3, restarts=16, best_only=True))[0]
+    b, _ = full.best()
+    assert bo.best() == full.best()
+    assert bo.json(b) == full.json(b).replace(str(full.summary(b).time_s), str(bo.summary(b).time_s)) or \
+        O.strip_time(bo.json(b)) == O.strip_time(full.json(b))
+    other = (b + 1) % 16
+    with pytest.raises(P.PlpError):
+        bo.json(other)
+
+
+@pytest.mark.parametrize("kw", [dict(eps=0.0, theta=None), dict(eps=0.3, theta=0.9, order="input"),
+                                dict(eps=0.7, theta=0.5, passes=2), dict(first_fit=True)])
+def test_plain_path_matches_oracle(kw):
+    text = synth.single_pass(1).to_thpack()
+    inst = P.Instance.parse(text)
+    passes = kw.pop("passes", 1)
+    r = P.run_plain(inst, seed=4, restarts=2, passes=passes, **kw)
+    oi = O.OInstance(text)
+    for k in range(2):
+        js, _, _ = O.run(oi, seed=4 + k, passes=passes, **kw)
+        assert O.strip_time(r.json(k)) == O.strip_time(js)
