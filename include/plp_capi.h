@@ -160,11 +160,15 @@ int plp_run_plain(const plp_instance* inst, const plp_run_opts* opts, plp_result
 int plp_create(size_t budget_bytes, int32_t device, plp_handle** out);
 void plp_destroy(plp_handle* h);
 
-/* Decoder tile for later solves on this handle: placed-box depth P, live-point
- * depth C (both per decoder, in shared memory) and decoders per CTA D (1..8);
- * 0 keeps the current value. Restarts that outgrow the tile are re-run with a
- * deeper one, so the tile affects speed only, never results. */
-int plp_set_tile(plp_handle* h, int32_t P, int32_t C, int32_t D);
+/* Decoder tile for later solves on this handle: placed-box depth P and
+ * live-point depth C (per decoder, in shared memory; C a multiple of 32),
+ * warps per decoder G, decoders per CTA D and minimum resident CTAs per SM M
+ * (which caps registers per thread at 65536 / (32 G D M)). (G, D, M) must be
+ * one of (1,2,1) (1,4,1) (1,4,4) (1,8,1) (1,8,2) (2,1,1) (2,2,1) (2,2,5)
+ * (2,4,1) (2,4,3) (4,1,1) (4,1,5) (4,1,6) (4,2,1) (4,2,3) (4,4,1) (8,1,1)
+ * (8,1,3) (8,2,1); 0 keeps the current value. Restarts that outgrow the tile
+ * are re-run with a deeper one, so the tile affects speed only, never results. */
+int plp_set_tile(plp_handle* h, int32_t P, int32_t C, int32_t G, int32_t D, int32_t M);
 
 /* Synchronous batched solve: every restart of every instance in one
  * persistent decoder launch (plus a FSR/selection launch), results copied to

@@ -90,13 +90,18 @@ void record(plp_handle* h, int status);
 struct TileConfig {
     int P = 128;       // placed-box tile depth per decoder
     int C = 384;       // live-point tile depth per decoder
-    int D = 4;         // decoders (warps) per CTA
+    int G = 1;         // warps per decoder
+    int D = 4;         // decoders per CTA
+    int M = 1;         // minimum resident CTAs per SM (register cap)
 };
 
 // Tiles only deepen: a retry that needed a deeper tile is remembered so the
 // next batch of this handle starts there.
 void remember_tile(TileConfig& keep, const TileConfig& used) {
-    if (used.P > keep.P || used.C > keep.C) keep = used;
+    keep.P = std::max(keep.P, used.P);
+    keep.C = std::max(keep.C, used.C);
+    while (keep.D > 1 && decoder_smem_bytes(keep.P, keep.C, 4096) * keep.D > 200 * 1024) keep.D >>= 1;
+    if (!decoder_config_supported(keep.G, keep.D, keep.M)) keep.M = 1;
 }
 
 constexpr int P_MAX = 2048;
@@ -112,7 +117,7 @@ struct Batch {
     std::vector<std::vector<TypeOrs>> inst_ors;
     std::vector<int2> work;
     long long n_slots = 0, n_places = 0;
-    int max_stride = 1, max_steps = 0;
+    int max_stride = 1, max_steps = 0, Hz = 0;
     bool multi_pass = false;
     // device
     char* d_mem = nullptr;
@@ -139,6 +144,7 @@ struct Batch {
         opts = op;
         desc.clear(); steps.clear(); types.clear(); work.clear(); inst_ors.clear();
         n_slots = 0; n_places = 0; max_stride = 1; max_steps = 0; multi_pass = false;
+        int maxH = 0;
         best_only = true;
         for (size_t i = 0; i < in.size(); i++) {
             const Instance& I = *in[i];
@@ -192,7 +198,10 @@ struct Batch {
             max_steps = std::max(max_steps, d.n_steps);
             multi_pass = multi_pass || o.passes > 1;
             best_only = best_only && o.best_only;
+            maxH = std::max(maxH, I.H);
         }
+        // top-z index: one u16 per height level 0 .. H + 1 (binary search above 4094)
+        Hz = maxH + 2 <= 4096 ? ((maxH + 2 + 7) & ~7) : 0;
         if (n_slots > INT_MAX / 2) return set_error(PLP_E_CAPACITY, "too many restarts in one batch");
         // longest instances first (dynamic scheduling then balances the tail)
         std::vector<int> order(in.size());
@@ -211,7 +220,7 @@ struct Batch {
     void plan(int sms, const TileConfig& t) {
         tile = t;
         int occ = 1;
-        if (decoder_occupancy(t.P, t.C, t.D, &occ) != cudaSuccess || occ < 1) occ = 1;
+        if (decoder_occupancy(t.P, t.C, Hz, t.G, t.D, t.M, &occ) != cudaSuccess || occ < 1) occ = 1;
         const long long need = (n_slots + t.D - 1) / t.D;
         ctas = (int)std::max(1LL, std::min<long long>(need, (long long)sms * occ));
         scratch_bytes = multi_pass ? (size_t)ctas * t.D * max_stride * 8 : 0;
@@ -330,15 +339,19 @@ static DecodeLaunch make_launch(const Batch& b, const TileConfig& t, const int2*
     L.n_work = n_work;
     L.work_next = reinterpret_cast<int*>(b.d_mem + b.o_next);
     L.err_flag = reinterpret_cast<int*>(b.d_mem + b.o_next + 8);
+    L.abort = reinterpret_cast<int*>(b.d_mem + b.o_next + 12);
     L.heads = reinterpret_cast<SlotHead*>(b.d_mem + b.o_heads);
     L.places = reinterpret_cast<unsigned long long*>(b.d_mem + b.o_places);
     L.scratch = reinterpret_cast<unsigned long long*>(b.d_mem + b.o_scratch);
     L.mt_init = b.mt_init;
     L.P = t.P;
     L.C = t.C;
+    L.Hz = b.Hz;
+    L.warps_per_decoder = t.G;
     L.decoders_per_cta = t.D;
+    L.min_blocks = t.M;
     int occ = 1;
-    if (decoder_occupancy(t.P, t.C, t.D, &occ) != cudaSuccess || occ < 1) occ = 1;
+    if (decoder_occupancy(t.P, t.C, b.Hz, t.G, t.D, t.M, &occ) != cudaSuccess || occ < 1) occ = 1;
     L.ctas = (int)std::max<long long>(1, std::min<long long>((n_work + t.D - 1) / t.D, (long long)sms * occ));
     // multi-pass scratch holds one placement row per resident decoder
     if (b.multi_pass) {
@@ -381,6 +394,10 @@ int batch_execute(Batch& b, cudaStream_t st, int sms, TileConfig& tile, ExecStat
             batch_release(b, st);
             return set_error(PLP_E_DEVICE, "decoder reported an RNG rejection-bound error");
         }
+        if (*reinterpret_cast<volatile int*>(b.h_flag) & (1 << ERR_SYNC)) {
+            batch_release(b, st);
+            return set_error(PLP_E_DEVICE, "decoder warps stopped meeting at a barrier (bounded wait gave up)");
+        }
         b.heads.resize(b.n_slots);
         e = cudaMemcpyAsync(b.heads.data(), b.d_mem + b.o_heads, b.n_slots * sizeof(SlotHead),
                             cudaMemcpyDeviceToHost, st);
@@ -400,8 +417,10 @@ int batch_execute(Batch& b, cudaStream_t st, int sms, TileConfig& tile, ExecStat
         if (grow_p) t.P = std::min(P_MAX, std::max(t.P * 2, 32));
         if (grow_c) t.C = std::min(C_MAX, t.C * 2);
         // deeper tiles: fewer decoders per CTA keeps one CTA within 227 KB
-        while (t.D > 1 && decoder_smem_bytes(t.P, t.C) * t.D > 200 * 1024) t.D >>= 1;
-        if (decoder_smem_bytes(t.P, t.C) > 227 * 1024) {
+        while (t.D > 1 && decoder_smem_bytes(t.P, t.C, b.Hz) * t.D > 200 * 1024) t.D >>= 1;
+        while (!decoder_config_supported(t.G, t.D, t.M) && t.D > 1) t.D >>= 1;
+        if (!decoder_config_supported(t.G, t.D, t.M)) t.M = 1;
+        if (decoder_smem_bytes(t.P, t.C, b.Hz) > 227 * 1024 || !decoder_config_supported(t.G, t.D, t.M)) {
             batch_release(b, st);
             return set_error(PLP_E_CAPACITY, "instance needs a larger tile than shared memory holds");
         }
@@ -968,9 +987,9 @@ void plp_destroy(plp_handle* h) {
     delete h;
 }
 
-int plp_set_tile(plp_handle* h, int32_t P, int32_t C, int32_t D) {
+int plp_set_tile(plp_handle* h, int32_t P, int32_t C, int32_t G, int32_t D, int32_t M) {
     if (!h) return set_error(PLP_E_INVALID, "plp_set_tile: null handle");
-    if (P < 0 || C < 0 || D < 0 || D > 8 || P > P_MAX || C > C_MAX) {
+    if (P < 0 || C < 0 || G < 0 || D < 0 || M < 0 || P > P_MAX || C > C_MAX || (C && C % 32)) {
         int s = set_error(PLP_E_INVALID, "plp_set_tile: out of range");
         record(h, s);
         return s;
@@ -980,8 +999,16 @@ int plp_set_tile(plp_handle* h, int32_t P, int32_t C, int32_t D) {
     TileConfig t = h->tile;
     if (P) t.P = P;
     if (C) t.C = C;
+    if (G) t.G = G;
     if (D) t.D = D;
-    if (decoder_smem_bytes(t.P, t.C) * t.D > 227 * 1024) {
+    if (M) t.M = M;
+    if (!decoder_config_supported(t.G, t.D, t.M)) {
+        int s = set_error(PLP_E_INVALID,
+                          "plp_set_tile: unsupported (warps per decoder, decoders per CTA, min CTAs per SM)");
+        record(h, s);
+        return s;
+    }
+    if (decoder_smem_bytes(t.P, t.C, 4096) * t.D > 227 * 1024) {
         int s = set_error(PLP_E_CAPACITY, "plp_set_tile: tile exceeds shared memory");
         record(h, s);
         return s;

@@ -41,6 +41,7 @@
 #include "feas_eval.cuh"
 
 #include <algorithm>
+#include <climits>
 #include <cstdio>
 #include <cstring>
 #include <vector>
@@ -50,11 +51,29 @@ namespace plpb {
 // ---------------------------------------------------------------------------
 // shared-memory layout of one decoder
 // ---------------------------------------------------------------------------
+// Scalars one decoder's warps exchange through shared memory.
+struct DecShared {
+    unsigned long long bar;   // mbarrier of the decoder's warps (G > 1)
+    int item;      // current work item
+    int nW;        // items in the filtered point list
+    int wnext;     // next unclaimed item
+    int best_w;    // smallest feasible item found so far
+    int full;      // random branch: every feasible pair is needed
+    int err;
+    int nc;        // live points
+    int nb;        // placed boxes
+    int pad[6];
+};
+static_assert(sizeof(DecShared) == 64, "DecShared layout");
+
 struct DecLayout {
-    int off_bx, off_bz, off_z2, off_bi, off_ca, off_cb, off_cm, bytes;
+    int off_bx, off_bz, off_z2, off_bi, off_ca, off_cb, off_cm, off_zt, off_sh, bytes;
+    __host__ __device__ int off_cc(int C) const { return off_cm + C; }   // chunk counts (int)
 };
 
-__host__ __device__ inline DecLayout dec_layout(int P, int C) {
+// P: placed-box depth, C: live-point depth, Hz: entries of the top-z index
+// (container height + 2; 0 = use binary search instead)
+__host__ __device__ inline DecLayout dec_layout(int P, int C, int Hz) {
     DecLayout l;
     int o = 624 * 4;                       // MT state
     o = (o + 15) & ~15;
@@ -64,18 +83,22 @@ __host__ __device__ inline DecLayout dec_layout(int P, int C) {
     l.off_bi = o;  o += 2 * P;             // placement index
     o = (o + 15) & ~15;
     l.off_ca = o;
-    // point buffers: 2 x C keys + C mask bytes; FSR overlays 18 bytes per box
-    int region = 9 * C;
+    // live points (4C), item list / survivor scratch (8C), item masks (C),
+    // per-chunk item counts (C / 8); FSR overlays 18 bytes per box
+    int region = 13 * C + C / 8 + 16;
     if (region < 18 * P + 32) region = 18 * P + 32;
     l.off_cb = o + 4 * C;
-    l.off_cm = o + 8 * C;
+    l.off_cm = o + 12 * C;
     o += region;
     o = (o + 15) & ~15;
+    l.off_zt = o;  o += 2 * Hz;            // u16: boxes with top < z
+    o = (o + 15) & ~15;
+    l.off_sh = o;  o += (int)sizeof(DecShared);
     l.bytes = o;
     return l;
 }
 
-int decoder_smem_bytes(int P, int C) { return dec_layout(P, C).bytes; }
+int decoder_smem_bytes(int P, int C, int Hz) { return dec_layout(P, C, Hz).bytes; }
 
 struct DecoderArgs {
     const InstDesc* __restrict__ inst;
@@ -85,13 +108,12 @@ struct DecoderArgs {
     int n_work;
     int* work_next;
     int* err_flag;
+    int* abort;
     SlotHead* heads;
     unsigned long long* places;
     unsigned long long* scratch;   // per resident warp: passes > 1
     const uint32_t* __restrict__ mt_init;
-    int P, C;
-    int dec_bytes;
-    int decoders_per_cta;
+    int P, C, Hz;
 };
 
 // ---------------------------------------------------------------------------
@@ -208,32 +230,402 @@ __device__ __forceinline__ double fsr_score_warp(const int4* bx, const int* bz, 
 }
 
 // ---------------------------------------------------------------------------
-// the persistent decoder kernel
+// the persistent decoder kernel: D decoders per CTA, G warps per decoder
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(128, 1) decoder_kernel(DecoderArgs a) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+// Barrier of one decoder's G warps: an mbarrier in shared memory that
+// completes a phase when each warp has arrived once. Every wait is bounded:
+// if it gives up, or another warp of the launch already gave up, the
+// launch-wide abort flag is set and the caller unwinds, so a broken
+// synchronisation ends the launch with ERR_SYNC instead of hanging the GPU.
+constexpr int SYNC_WAIT_LIMIT = 1 << 20;
+
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+    const unsigned a = (unsigned)__cvta_generic_to_shared(bar);
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(a), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(unsigned long long* bar) {
+    const unsigned a = (unsigned)__cvta_generic_to_shared(bar);
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(a) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+    const unsigned a = (unsigned)__cvta_generic_to_shared(bar);
+    unsigned ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(a), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+template <int G>
+struct GroupSync {
+    unsigned long long* bar;
+    int* abort;
+    unsigned phase;
+    // returns false when the launch is aborting (the caller must return)
+    __device__ __forceinline__ bool operator()(int lane) {
+        __syncwarp();
+        if (G == 1) return true;
+        if (lane == 0) mbar_arrive(bar);
+        bool ok = true;
+        for (int k = 0; !mbar_try_wait(bar, phase); k++) {
+            if (k >= SYNC_WAIT_LIMIT || *reinterpret_cast<volatile int*>(abort)) {
+                ok = false;
+                break;
+            }
+        }
+        phase ^= 1u;
+        ok = __all_sync(FULL, ok);
+        if (!ok && lane == 0) atomicExch(abort, 1);
+        return ok;
+    }
+};
+
+// first box with top >= z, and first box with top > z
+__device__ __forceinline__ int box_start(const unsigned short* zt, const int* z2, int nb, int z) {
+    return zt ? (int)zt[z] : lower_bound_top(z2, nb, z);
+}
+
+// Per-step orientation data (identical in every warp of a decoder).
+struct StepOrs {
+    int no;
+    int ow[6], od[6], oh[6], wd[6];
+    int wmax, dmax, hmax;   // largest edge along x, y, z over the orientations
+};
+
+// One decoder's G warps evaluate the filtered points W[start .. nW): warp g
+// takes points start + g, start + g + G, ...; inside a warp each lane tests
+// one placed box, so a point's boxes are checked 32 at a time with coalesced
+// loads and the per-box results are combined with warp reductions.
+//   C3 (z > 0): integer contact areas of the boxes whose top is z, summed
+//               with __reduce_add_sync; lane o then applies the FP64 ratio
+//               test of orientation o.
+//   C1:         boxes whose top is above z; an orientation is blocked when a
+//               box overlaps it; blocked sets are OR-reduced per 32 boxes and
+//               the scan stops once every orientation is blocked.
+// Greedy mode stops at the smallest feasible item (sh->best_w); the mask of
+// every evaluated item goes to wmask.
+// Item of the filtered point list: x = point key, y = orientation mask
+// (bits 0-5) | first box with top >= z (bits 8-19) | first box with top > z
+// (bits 20-31). Box indices refer to the top-sorted tables of this step.
+__device__ __forceinline__ uint2 make_item(uint32_t key, unsigned m, int jlo, int jsup) {
+    return make_uint2(key, m | ((unsigned)jlo << 8) | ((unsigned)jsup << 20));
+}
+
+// One decoder's G warps evaluate the filtered points W[start .. nW) in
+// chunks of 32 (chunk k by warp k % G), one lane per point. All lanes walk the
+// top-sorted boxes in lockstep, so every box is one shared-memory broadcast:
+//   support loop: boxes whose top is the height of some lane's point; each
+//                 lane adds the integer contact areas of the boxes with top ==
+//                 its z, then applies the FP64 ratio test (C3);
+//   C1 loop:      boxes above, from the lowest start of the chunk, until every
+//                 lane's orientations are blocked.
+// Greedy mode stops at the first chunk with a feasible point and records the
+// smallest feasible item in sh->best_w; every evaluated item's mask goes to
+// wmask.
+template <int G, bool GREEDY>
+__device__ __forceinline__ void scan_points(DecShared* sh, const uint2* W, unsigned char* wmask,
+                                            const int4* bx, const int* bzs, int nb, const StepOrs& S,
+                                            uint32_t xmask, uint32_t ymask, int xb, int xyb, int g,
+                                            int lane, int start) {
+    const int nW = sh->nW;
+    for (int cb = start + 32 * g; cb < nW; cb += 32 * G) {
+        if (GREEDY && G > 1 && cb > *reinterpret_cast<volatile int*>(&sh->best_w)) break;
+        const int w = cb + lane;
+        const uint2 e = w < nW ? W[w] : make_uint2(0, 0);
+        unsigned alive = e.y & 0x3fu;
+        const int jlo = (int)((e.y >> 8) & 0xfffu), jsup = (int)(e.y >> 20);
+        const int x = (int)(e.x & xmask), y = (int)((e.x >> xb) & ymask), z = (int)(e.x >> xyb);
+        const bool sup = alive && jsup > jlo;                            // z > 0
+        const int slo = __reduce_min_sync(FULL, sup ? jlo : INT_MAX);
+        const int shi = __reduce_max_sync(FULL, sup ? jsup : 0);
+        if (slo < shi) {                                                 // C3 support
+            int a0 = 0, a1 = 0, a2 = 0, a3 = 0, a4 = 0, a5 = 0;
+            for (int j0 = slo; j0 < shi; j0 += 4) {
+                int4 bb[4];
+#pragma unroll
+                for (int u = 0; u < 4; u++) bb[u] = j0 + u < shi ? bx[j0 + u] : make_int4(0, 0, 0, 0);
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    const int j = j0 + u;
+                    const int4 b = bb[u];
+                    if (sup && j >= jlo && j < jsup) {
+#define PLP_ACC(o, av)                                                   \
+    {                                                                    \
+        const int ox = min(x + S.ow[o], b.z) - max(x, b.x);              \
+        const int oy = min(y + S.od[o], b.w) - max(y, b.y);              \
+        if (ox > 0 && oy > 0) av += ox * oy;                             \
+    }
+                        PLP_ACC(0, a0) PLP_ACC(1, a1) PLP_ACC(2, a2) PLP_ACC(3, a3) PLP_ACC(4, a4) PLP_ACC(5, a5)
+#undef PLP_ACC
+                    }
+                }
+            }
+            if (sup) {
+                // (double)s / (double)(w*d) < 0.5 fails the orientation
+                const int av[6] = {a0, a1, a2, a3, a4, a5};
+#pragma unroll
+                for (int o = 0; o < 6; o++)
+                    if (((alive >> o) & 1u) && (double)av[o] / (double)S.wd[o] < 0.5) alive &= ~(1u << o);
+            }
+        }
+        const int clo = __reduce_min_sync(FULL, alive ? jsup : INT_MAX);
+        // C1 overlap, 4 boxes per round: loads first, then a cheap "near"
+        // test per box (ahead of the point and within the largest edge on each
+        // axis); only boxes near some lane get the per-orientation test. Boxes
+        // past nb read as {0,0,0,0}, which is never near (x >= 0).
+        for (int j0 = clo; j0 < nb; j0 += 4) {
+            int4 bb[4];
+            int bz[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const bool in = j0 + u < nb;
+                bb[u] = in ? bx[j0 + u] : make_int4(0, 0, 0, 0);
+                bz[u] = in ? bzs[j0 + u] : 0;
+            }
+            unsigned near = 0;
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const int4 b = bb[u];
+                const bool nu = alive && j0 + u >= jsup && x < b.z && y < b.w && b.x < x + S.wmax &&
+                                b.y < y + S.dmax && bz[u] < z + S.hmax;
+                near |= (nu ? 1u : 0u) << u;
+            }
+            unsigned todo = __reduce_or_sync(FULL, near);
+            while (todo) {
+                const int u = __ffs(todo) - 1;
+                todo &= todo - 1;
+                if ((near >> u) & 1u) {
+                    const int4 b = bb[u];
+                    const int bzu = bz[u];
+#pragma unroll
+                    for (int o = 0; o < 6; o++)
+                        if (b.x < x + S.ow[o] && b.y < y + S.od[o] && bzu < z + S.oh[o]) alive &= ~(1u << o);
+                }
+            }
+            if (!__any_sync(FULL, alive != 0)) break;
+        }
+        if (w < nW) wmask[w] = (unsigned char)alive;
+        if (GREEDY) {
+            const unsigned bal = __ballot_sync(FULL, alive != 0);
+            if (bal) {
+                if (lane == 0) atomicMin(&sh->best_w, cb + __ffs(bal) - 1);
+                break;
+            }
+        }
+    }
+}
+
+// Filtered item of one live point (C2 mask, and above the floor at least one
+// box top at its height), or m = 0.
+__device__ __forceinline__ uint2 filter_point(uint32_t key, const StepOrs& S, int L, int W, int H,
+                                              uint32_t xmask, uint32_t ymask, int xb, int xyb,
+                                              const unsigned short* zt, const int* z2s, int nb) {
+    const int x = (int)(key & xmask), y = (int)((key >> xb) & ymask), z = (int)(key >> xyb);
+    unsigned m = 0;
+#pragma unroll
+    for (int o = 0; o < 6; o++)
+        if (o < S.no && x + S.ow[o] <= L && y + S.od[o] <= W && z + S.oh[o] <= H) m |= 1u << o;
+    if (!m) return make_uint2(0, 0);
+    const int jlo = box_start(zt, z2s, nb, z);
+    const int jsup = z > 0 ? box_start(zt, z2s, nb, z + 1) : jlo;
+    if (z > 0 && jsup == jlo) return make_uint2(0, 0);   // nothing supports a box at this height
+    return make_item(key, m, jlo, jsup);
+}
+
+// Warp 0 of a decoder: pick the pair, place the box, update the live points,
+// the top-sorted box tables and the top-z index. Returns a DecodeErr.
+__device__ __forceinline__ int place_step(DecShared* sh, const StepOrs& S, int t, int best, bool full,
+                                          uint32_t* mt, int& mpos, uint32_t* candA, uint32_t* candB,
+                                          const uint2* W,
+                                          const unsigned char* cmask, int4* bx, int* bzs, int* z2s,
+                                          unsigned short* bis, unsigned short* zt, int Hz, int& nc,
+                                          int& nb, int P, int C, uint32_t xmask, uint32_t ymask, int xb,
+                                          int xyb, unsigned long long* pass_out, long long& vol, int lane) {
+    int pick_w = best;
+    int pick_oi = __ffs(cmask[best]) - 1;
+    if (full) {
+        const int nW = sh->nW;
+        int count = 0;
+        for (int i = best + lane; i < nW; i += 32) count += __popc(cmask[i]);
+        count = __reduce_add_sync(FULL, count);
+        const int idx = mt_randrange(mt, mpos, lane, count);
+        if (idx < 0) return ERR_RNG;
+        // idx-th feasible pair in (point, orientation) order
+        int run = 0;
+        for (int cb = best; cb < nW; cb += 32) {
+            const int i = cb + lane;
+            const unsigned m = i < nW ? cmask[i] : 0u;
+            const int c = __popc(m);
+            int inc = c;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const int v = __shfl_up_sync(FULL, inc, d);
+                if (lane >= d) inc += v;
+            }
+            const int tot = __shfl_sync(FULL, inc, 31);
+            if (idx < run + tot) {
+                const unsigned hit = __ballot_sync(FULL, idx < run + inc);
+                const int l = __ffs(hit) - 1;
+                const int excl = __shfl_sync(FULL, inc - c, l);
+                const unsigned ml = __shfl_sync(FULL, m, l);
+                pick_w = cb + l;
+                pick_oi = __fns(ml, 0, idx - run - excl + 1);
+                break;
+            }
+            run += tot;
+        }
+    }
+    const uint32_t pkey = W[pick_w].x;
+    __syncwarp();   // every lane has read the item list before candB is overwritten
+    const int px = (int)(pkey & xmask), py = (int)((pkey >> xb) & ymask), pz = (int)(pkey >> xyb);
+    int pw = 0, pd = 0, ph = 0;
+#pragma unroll
+    for (int o = 0; o < 6; o++)
+        if (o == pick_oi) { pw = S.ow[o]; pd = S.od[o]; ph = S.oh[o]; }
+    const int px2 = px + pw, py2 = py + pd, pz2 = pz + ph;
+    if (nb >= P) return ERR_BOX_CAP;
+    if (lane == 0) pass_out[nb] = pack_place(px, py, pz, pick_oi, t);
+    vol += 1LL * pw * pd * ph;
+    // corners of the new box covered by an already placed box
+    unsigned cov = 1u;   // corner 0 = (px, py, pz): covered by the new box
+    for (int jj = lane; jj < nb; jj += 32) {
+        const int4 b = bx[jj];
+        const int bzb = bzs[jj], bzt = z2s[jj];
+        const unsigned xin = (b.x <= px && px < b.z ? 1u : 0u) | (b.x <= px2 && px2 < b.z ? 2u : 0u);
+        const unsigned yin = (b.y <= py && py < b.w ? 1u : 0u) | (b.y <= py2 && py2 < b.w ? 2u : 0u);
+        const unsigned zin = (bzb <= pz && pz < bzt ? 1u : 0u) | (bzb <= pz2 && pz2 < bzt ? 2u : 0u);
+#pragma unroll
+        for (int c = 0; c < 8; c++)
+            if (((xin >> (c & 1)) & (yin >> ((c >> 1) & 1)) & (zin >> (c >> 2))) & 1u) cov |= 1u << c;
+    }
+    cov = __reduce_or_sync(FULL, cov);
+    // survivors (points not covered by the new box), compacted into candB
+    // (the item list it held is no longer read: the pick was taken above)
+    int ns = 0;
+    for (int cb = 0; cb < nc; cb += 32) {
+        const int i = cb + lane;
+        bool keep = false;
+        uint32_t key = 0;
+        if (i < nc) {
+            key = candA[i];
+            const int x = (int)(key & xmask), y = (int)((key >> xb) & ymask), z = (int)(key >> xyb);
+            keep = !(px <= x && x < px2 && py <= y && y < py2 && pz <= z && z < pz2);
+        }
+        const unsigned bal = __ballot_sync(FULL, keep);
+        if (keep) candB[ns + __popc(bal & lanemask_lt())] = key;
+        ns += __popc(bal);
+    }
+    __syncwarp();
+    // new corners, in index order c = (cz << 2) | (cy << 1) | cx, which is their (z, y, x) order
+    uint32_t ck = 0;
+    int rank = 0;
+    bool isnew = false;
+    if (lane < 8 && !((cov >> lane) & 1u)) {
+        const int cx = (lane & 1) ? px2 : px, cy = (lane & 2) ? py2 : py, cz = (lane & 4) ? pz2 : pz;
+        ck = ((uint32_t)cz << xyb) | ((uint32_t)cy << xb) | (uint32_t)cx;
+        int lo = 0, n = ns;
+        while (n > 0) {
+            const int half = n >> 1;
+            if (candB[lo + half] < ck) { lo += half + 1; n -= half + 1; }
+            else n = half;
+        }
+        rank = lo;
+        isnew = !(lo < ns && candB[lo] == ck);
+    }
+    const unsigned newm = __ballot_sync(FULL, isnew);
+    const int nnew = ns + __popc(newm);
+    if (nnew > C) return ERR_CAND_CAP;
+    uint32_t ckk[8];
+#pragma unroll
+    for (int c = 0; c < 8; c++) ckk[c] = __shfl_sync(FULL, ck, c);
+    for (int cb = 0; cb < ns; cb += 32) {
+        const int i = cb + lane;
+        if (i < ns) {
+            const uint32_t key = candB[i];
+            int off = 0;
+#pragma unroll
+            for (int c = 0; c < 8; c++) off += ((newm >> c) & 1u) && ckk[c] < key;
+            candA[i + off] = key;
+        }
+    }
+    if (isnew) candA[rank + __popc(newm & ((1u << lane) - 1u))] = ck;
+    nc = nnew;
+    // insert the box into the top-sorted tables (after equal tops)
+    int ip;
+    {
+        int lo = 0, n = nb;
+        while (n > 0) {
+            const int half = n >> 1;
+            if (z2s[lo + half] <= pz2) { lo += half + 1; n -= half + 1; }
+            else n = half;
+        }
+        ip = lo;
+    }
+    for (int hi = nb; hi > ip; hi -= 32) {
+        const int i = hi - 1 - lane;
+        int4 vb = make_int4(0, 0, 0, 0);
+        int vz = 0, vt = 0;
+        unsigned short vi = 0;
+        const bool mv = i >= ip;
+        if (mv) { vb = bx[i]; vz = bzs[i]; vt = z2s[i]; vi = bis[i]; }
+        __syncwarp();
+        if (mv) { bx[i + 1] = vb; bzs[i + 1] = vz; z2s[i + 1] = vt; bis[i + 1] = vi; }
+        __syncwarp();
+    }
+    if (lane == 0) {
+        bx[ip] = make_int4(px, py, px2, py2);
+        bzs[ip] = pz;
+        z2s[ip] = pz2;
+        bis[ip] = (unsigned short)nb;
+    }
+    if (zt)
+        for (int zz = pz2 + 1 + lane; zz < Hz; zz += 32) zt[zz]++;
+    nb++;
+    __syncwarp();
+    return ERR_NONE;
+}
+
+template <int G>
+__device__ __forceinline__ void decoder_body(const DecoderArgs& a, unsigned char* base, int dec,
+                                             int gdec) {
     const int lane = threadIdx.x & 31;
-    const int wid = threadIdx.x >> 5;
-    const DecLayout lay = dec_layout(a.P, a.C);
-    unsigned char* base = smem_raw + (size_t)wid * a.dec_bytes;
+    const int g = (threadIdx.x >> 5) % G;
+    const DecLayout lay = dec_layout(a.P, a.C, a.Hz);
     uint32_t* mt = reinterpret_cast<uint32_t*>(base);
     int4* bx = reinterpret_cast<int4*>(base + lay.off_bx);
     int* bzs = reinterpret_cast<int*>(base + lay.off_bz);
     int* z2s = reinterpret_cast<int*>(base + lay.off_z2);
     unsigned short* bis = reinterpret_cast<unsigned short*>(base + lay.off_bi);
     uint32_t* candA = reinterpret_cast<uint32_t*>(base + lay.off_ca);
-    uint32_t* candB = reinterpret_cast<uint32_t*>(base + lay.off_cb);
-    unsigned char* cmask = base + lay.off_cm;
-    const int gwarp = blockIdx.x * a.decoders_per_cta + wid;
+    uint32_t* candB = reinterpret_cast<uint32_t*>(base + lay.off_cb);   // survivor scratch
+    uint2* Wl = reinterpret_cast<uint2*>(base + lay.off_cb);             // item list (same space)
+    unsigned char* cmask = base + lay.off_cm;                             // item masks
+    int* ccount = reinterpret_cast<int*>(base + lay.off_cc(a.C));         // per-chunk item counts
+    unsigned short* zt = a.Hz ? reinterpret_cast<unsigned short*>(base + lay.off_zt) : nullptr;
+    DecShared* sh = reinterpret_cast<DecShared*>(base + lay.off_sh);
+    GroupSync<G> sync{&sh->bar, a.abort, 0u};
+#define PLP_SYNC()                        \
+    if (!sync(lane)) {                    \
+        if (lane == 0) atomicOr(a.err_flag, 1 << ERR_SYNC); \
+        return;                           \
+    }
 
     for (;;) {
-        int item = 0;
-        if (lane == 0) item = atomicAdd(a.work_next, 1);
-        item = __shfl_sync(FULL, item, 0);
+        if (*reinterpret_cast<volatile int*>(a.abort)) return;
+        if (g == 0 && lane == 0) sh->item = atomicAdd(a.work_next, 1);
+        PLP_SYNC()
+        const int item = sh->item;
+        PLP_SYNC()   // everyone has the item before it can change
         if (item >= a.n_work) break;
-        const int2 w = a.work[item];
-        const InstDesc I = a.inst[w.x];
-        const int restart = w.y;
+        const int2 wk = a.work[item];
+        const InstDesc I = a.inst[wk.x];
+        const int restart = wk.y;
         const int slot = I.slot_base + restart;
         const int L = I.L, W = I.W, H = I.H;
         const uint32_t xmask = (1u << I.xb) - 1u, ymask = (1u << I.yb) - 1u;
@@ -241,13 +633,12 @@ __global__ void __launch_bounds__(128, 1) decoder_kernel(DecoderArgs a) {
         const bool randomized = !(I.first_fit || I.eps == 0.0);
         unsigned long long* best_out = a.places + I.place_off + (long long)restart * I.place_stride;
         unsigned long long* pass_out =
-            I.passes > 1 ? a.scratch + (long long)gwarp * I.place_stride : best_out;
-
-        long long s = I.seed + restart;
-        const unsigned long long sabs = (unsigned long long)(s < 0 ? -s : s);
-        mt_seed_warp(mt, sabs, a.mt_init, lane);
-        int mpos = 624;
-
+            I.passes > 1 ? a.scratch + (long long)gdec * I.place_stride : best_out;
+        int mpos = 624;   // RNG position (warp 0)
+        if (g == 0) {
+            const long long sd = I.seed + restart;
+            mt_seed_warp(mt, (unsigned long long)(sd < 0 ? -sd : sd), a.mt_init, lane);
+        }
         int err = ERR_NONE;
         bool have_acc = false, have_any = false;
         long long best_vol = 0;
@@ -255,214 +646,147 @@ __global__ void __launch_bounds__(128, 1) decoder_kernel(DecoderArgs a) {
         double best_score = 0.0;
 
         for (int pass = 0; pass < I.passes && err == ERR_NONE; pass++) {
-            int nb = 0, nc = 1;
+            int nb = 0, nc = 1;   // warp 0's copies are authoritative
             long long vol = 0;
-            if (lane == 0) candA[0] = 0u;
-            __syncwarp();
+            if (zt)
+                for (int i = threadIdx.x % (32 * G); i < a.Hz; i += 32 * G) zt[i] = 0;
+            if (g == 0 && lane == 0) {
+                candA[0] = 0u;
+                sh->err = ERR_NONE;
+                sh->nc = 1;
+                sh->nb = 0;
+            }
             for (int st = 0; st < I.n_steps; st++) {
                 const int t = a.step_type[I.step_off + st];
                 const TypeOrs& T = a.types[I.type_off + t];
-                const int no = T.n;
-                if (no == 0) continue;
-                int ow[6], od[6], oh[6];
+                StepOrs S;
+                S.no = T.n;
+                if (S.no == 0) continue;
+                S.wmax = S.dmax = S.hmax = 0;
 #pragma unroll
                 for (int o = 0; o < 6; o++) {
-                    ow[o] = T.w[o];
-                    od[o] = T.d[o];
-                    oh[o] = T.h[o];
+                    S.ow[o] = T.w[o];
+                    S.od[o] = T.d[o];
+                    S.oh[o] = T.h[o];
+                    S.wd[o] = S.ow[o] * S.od[o];
+                    S.wmax = max(S.wmax, S.ow[o]);
+                    S.dmax = max(S.dmax, S.od[o]);
+                    S.hmax = max(S.hmax, S.oh[o]);
                 }
-                const Boxes B{bx, bzs, z2s, nb};
-                // scan live points in order: greedy stops at the first chunk
-                // holding a feasible pair; the random branch scans on and
-                // records every point's mask
-                int first_ci = -1, first_oi = 0, count = 0;
-                bool full = false;
-                for (int cb = 0; cb < nc; cb += 32) {
-                    const int ci = cb + lane;
-                    unsigned m = 0;
-                    if (ci < nc) {
-                        const uint32_t key = candA[ci];
-                        m = eval_point<int>((int)(key & xmask), (int)((key >> xb) & ymask),
-                                       (int)(key >> xyb), ow, od, oh, no, L, W, H, B);
-                    }
-                    if (!full) {
-                        const unsigned bal = __ballot_sync(FULL, m != 0);
-                        if (!bal) continue;
-                        const int l = __ffs(bal) - 1;
-                        first_ci = cb + l;
-                        first_oi = __ffs(__shfl_sync(FULL, m, l)) - 1;
-                        if (!randomized) break;
-                        const double u = mt_random(mt, mpos, lane);
-                        if (u < 1.0 - I.eps) break;
-                        full = true;
-                    }
-                    if (ci < nc) cmask[ci] = (unsigned char)m;
-                    count += __reduce_add_sync(FULL, __popc(m));
-                }
-                if (first_ci < 0) continue;               // no feasible pair: skip this copy
-                int pick_ci = first_ci, pick_oi = first_oi;
-                if (full) {
-                    __syncwarp();
-                    const int idx = mt_randrange(mt, mpos, lane, count);
-                    if (idx < 0) { err = ERR_RNG; break; }
-                    // idx-th feasible pair in (point, orientation) order
-                    int run = 0;
-                    const int cb0 = first_ci & ~31;
-                    for (int cb = cb0; cb < nc; cb += 32) {
+                PLP_SYNC()                 // A: previous step's tables are final
+                if (sh->err != ERR_NONE) break;
+                nc = sh->nc;
+                nb = sh->nb;
+                // filter: points with an orientation inside the container and,
+                // above the floor, at least one box top at their height
+                if (G == 1) {
+                    int nW = 0;
+                    for (int cb = 0; cb < nc; cb += 32) {
                         const int ci = cb + lane;
-                        const unsigned m = ci < nc && ci >= first_ci ? cmask[ci] : 0u;
-                        const int c = __popc(m);
-                        int inc = c;
-#pragma unroll
-                        for (int d = 1; d < 32; d <<= 1) {
-                            const int v = __shfl_up_sync(FULL, inc, d);
-                            if (lane >= d) inc += v;
-                        }
-                        const int tot = __shfl_sync(FULL, inc, 31);
-                        if (idx < run + tot) {
-                            const unsigned hit = __ballot_sync(FULL, idx < run + inc);
-                            const int l = __ffs(hit) - 1;
-                            const int excl = __shfl_sync(FULL, inc - c, l);
-                            const unsigned ml = __shfl_sync(FULL, m, l);
-                            pick_ci = cb + l;
-                            pick_oi = __fns(ml, 0, idx - run - excl + 1);
-                            break;
-                        }
-                        run += tot;
+                        const uint2 it = ci < nc ? filter_point(candA[ci], S, L, W, H, xmask, ymask, xb,
+                                                                xyb, zt, z2s, nb)
+                                                 : make_uint2(0, 0);
+                        const bool keep = (it.y & 0x3fu) != 0;
+                        const unsigned bal = __ballot_sync(FULL, keep);
+                        if (keep) Wl[nW + __popc(bal & lanemask_lt())] = it;
+                        nW += __popc(bal);
                     }
-                }
-                // ---- place the box ----
-                const uint32_t pkey = candA[pick_ci];
-                const int px = (int)(pkey & xmask), py = (int)((pkey >> xb) & ymask),
-                          pz = (int)(pkey >> xyb);
-                int pw = 0, pd = 0, ph = 0;
-#pragma unroll
-                for (int o = 0; o < 6; o++)
-                    if (o == pick_oi) { pw = ow[o]; pd = od[o]; ph = oh[o]; }
-                const int px2 = px + pw, py2 = py + pd, pz2 = pz + ph;
-                if (nb >= a.P) { err = ERR_BOX_CAP; break; }
-                if (lane == 0) pass_out[nb] = pack_place(px, py, pz, pick_oi, t);
-                vol += 1LL * pw * pd * ph;
-
-                // ---- live-point update ----
-                // corners of the new box covered by an already placed box
-                unsigned cov = 1u;   // corner 0 = (px, py, pz) is covered by the new box
-                for (int j = lane; j < nb; j += 32) {
-                    const int4 b = bx[j];
-                    const int bzb = bzs[j], bzt = z2s[j];
-                    const unsigned xin = (b.x <= px && px < b.z ? 1u : 0u) | (b.x <= px2 && px2 < b.z ? 2u : 0u);
-                    const unsigned yin = (b.y <= py && py < b.w ? 1u : 0u) | (b.y <= py2 && py2 < b.w ? 2u : 0u);
-                    const unsigned zin = (bzb <= pz && pz < bzt ? 1u : 0u) | (bzb <= pz2 && pz2 < bzt ? 2u : 0u);
-#pragma unroll
-                    for (int c = 0; c < 8; c++)
-                        if (((xin >> (c & 1)) & (yin >> ((c >> 1) & 1)) & (zin >> (c >> 2))) & 1u)
-                            cov |= 1u << c;
-                }
-                cov = __reduce_or_sync(FULL, cov);
-                // survivors: points not covered by the new box, compacted into candB
-                int ns = 0;
-                for (int cb = 0; cb < nc; cb += 32) {
-                    const int i = cb + lane;
-                    bool keep = false;
-                    uint32_t key = 0;
-                    if (i < nc) {
-                        key = candA[i];
-                        const int x = (int)(key & xmask), y = (int)((key >> xb) & ymask),
-                                  z = (int)(key >> xyb);
-                        keep = !(px <= x && x < px2 && py <= y && y < py2 && pz <= z && z < pz2);
+                    if (lane == 0) {
+                        sh->nW = nW;
+                        sh->best_w = INT_MAX;
                     }
-                    const unsigned bal = __ballot_sync(FULL, keep);
-                    if (keep) candB[ns + __popc(bal & lanemask_lt())] = key;
-                    ns += __popc(bal);
-                }
-                __syncwarp();
-                // new corners: sorted by index c = (cz << 2) | (cy << 1) | cx,
-                // which is also their (z, y, x) order
-                uint32_t ck = 0;
-                int rank = 0;
-                bool isnew = false;
-                if (lane < 8 && !((cov >> lane) & 1u)) {
-                    const int cx = (lane & 1) ? px2 : px, cy = (lane & 2) ? py2 : py,
-                              cz = (lane & 4) ? pz2 : pz;
-                    ck = ((uint32_t)cz << xyb) | ((uint32_t)cy << xb) | (uint32_t)cx;
-                    int lo = 0, n = ns;
-                    while (n > 0) {
-                        const int half = n >> 1;
-                        if (candB[lo + half] < ck) { lo += half + 1; n -= half + 1; }
-                        else n = half;
+                } else {
+                    // two passes over chunks of 32 points (chunk c by warp c % G):
+                    // count, then write at the chunk's prefix offset
+                    const int nch = (nc + 31) >> 5;
+                    for (int c = g; c < nch; c += G) {
+                        const int ci = c * 32 + lane;
+                        const uint2 it = ci < nc ? filter_point(candA[ci], S, L, W, H, xmask, ymask, xb,
+                                                                xyb, zt, z2s, nb)
+                                                 : make_uint2(0, 0);
+                        const unsigned bal = __ballot_sync(FULL, (it.y & 0x3fu) != 0);
+                        if (lane == 0) ccount[c] = __popc(bal);
                     }
-                    rank = lo;
-                    isnew = !(lo < ns && candB[lo] == ck);
-                }
-                const unsigned newm = __ballot_sync(FULL, isnew);
-                const int nnew = ns + __popc(newm);
-                if (nnew > a.C) { err = ERR_CAND_CAP; break; }
-                uint32_t ckk[8];
-#pragma unroll
-                for (int c = 0; c < 8; c++) ckk[c] = __shfl_sync(FULL, ck, c);
-                for (int cb = 0; cb < ns; cb += 32) {
-                    const int i = cb + lane;
-                    if (i < ns) {
-                        const uint32_t key = candB[i];
+                    PLP_SYNC()
+                    // pass 2: offset of chunk c = sum of the counts before it (read only)
+                    for (int c = g; c < nch; c += G) {
                         int off = 0;
-#pragma unroll
-                        for (int c = 0; c < 8; c++) off += ((newm >> c) & 1u) && ckk[c] < key;
-                        candA[i + off] = key;
+                        for (int k = lane; k < c; k += 32) off += ccount[k];
+                        off = __reduce_add_sync(FULL, off);
+                        const int ci = c * 32 + lane;
+                        const uint2 it = ci < nc ? filter_point(candA[ci], S, L, W, H, xmask, ymask, xb,
+                                                                xyb, zt, z2s, nb)
+                                                 : make_uint2(0, 0);
+                        const bool keep = (it.y & 0x3fu) != 0;
+                        const unsigned bal = __ballot_sync(FULL, keep);
+                        if (keep) Wl[off + __popc(bal & lanemask_lt())] = it;
+                    }
+                    int run = 0;
+                    if (g == 0) {
+                        for (int k = lane; k < nch; k += 32) run += ccount[k];
+                        run = __reduce_add_sync(FULL, run);
+                    }
+                    if (g == 0 && lane == 0) {
+                        sh->nW = run;
+                        sh->best_w = INT_MAX;
                     }
                 }
-                if (isnew) candA[rank + __popc(newm & ((1u << lane) - 1u))] = ck;
-                nc = nnew;
-                // insert the box into the top-z-sorted tables (after equal tops)
-                int ip = 0;
-                {
-                    int lo = 0, n = nb;
-                    while (n > 0) {
-                        const int half = n >> 1;
-                        if (z2s[lo + half] <= pz2) { lo += half + 1; n -= half + 1; }
-                        else n = half;
+                PLP_SYNC()                 // B
+                if (sh->nW == 0) continue;             // no feasible pair: skip this copy
+                scan_points<G, true>(sh, Wl, cmask, bx, bzs, nb, S, xmask, ymask, xb, xyb, g, lane, 0);
+                PLP_SYNC()                 // C
+                if (g == 0) {                          // random() only once a pair is feasible
+                    const int best = sh->best_w;
+                    int full = 0;
+                    if (best != INT_MAX && randomized) full = mt_random(mt, mpos, lane) >= 1.0 - I.eps;
+                    if (lane == 0) sh->full = full;
+                }
+                PLP_SYNC()                 // D
+                const int best = sh->best_w;
+                if (best == INT_MAX) continue;
+                const bool full = sh->full != 0;
+                if (full) {
+                    scan_points<G, false>(sh, Wl, cmask, bx, bzs, nb, S, xmask, ymask, xb, xyb, g, lane,
+                                          best + 1);
+                    PLP_SYNC()             // E
+                }
+                if (g == 0) {
+                    const int e = place_step(sh, S, t, best, full, mt, mpos, candA, candB, Wl, cmask, bx, bzs,
+                                             z2s, bis, zt, a.Hz, nc, nb, a.P, a.C, xmask, ymask, xb, xyb,
+                                             pass_out, vol, lane);
+                    if (lane == 0) {
+                        sh->nc = nc;
+                        sh->nb = nb;
+                        if (e != ERR_NONE) sh->err = e;
                     }
-                    ip = lo;
                 }
-                for (int hi = nb; hi > ip; hi -= 32) {
-                    const int i = hi - 1 - lane;
-                    int4 vb = make_int4(0, 0, 0, 0);
-                    int vz = 0, vt = 0;
-                    unsigned short vi = 0;
-                    const bool mv = i >= ip;
-                    if (mv) { vb = bx[i]; vz = bzs[i]; vt = z2s[i]; vi = bis[i]; }
-                    __syncwarp();
-                    if (mv) { bx[i + 1] = vb; bzs[i + 1] = vz; z2s[i + 1] = vt; bis[i + 1] = vi; }
-                    __syncwarp();
+            }
+            PLP_SYNC()
+            err = sh->err;
+            nb = sh->nb;
+            if (err != ERR_NONE) break;
+            // score the pass and keep the selected one (warp 0)
+            if (g == 0) {
+                const double score = fsr_score_warp(bx, bzs, z2s, bis, nb, I.mu,
+                                                    reinterpret_cast<char*>(candA), lane, nullptr);
+                const bool acc = !I.has_theta || score >= I.theta;
+                bool take;
+                if (acc) take = !have_acc || vol > best_vol || (vol == best_vol && nb > best_n);
+                else take = !have_acc && (!have_any || vol > best_vol || (vol == best_vol && nb > best_n));
+                if (take) {
+                    best_vol = vol;
+                    best_n = nb;
+                    best_score = score;
+                    if (pass_out != best_out)
+                        for (int i = lane; i < nb; i += 32) best_out[i] = pass_out[i];
                 }
-                if (lane == 0) {
-                    bx[ip] = make_int4(px, py, px2, py2);
-                    bzs[ip] = pz;
-                    z2s[ip] = pz2;
-                    bis[ip] = (unsigned short)nb;
-                }
-                nb++;
+                have_any = true;
+                have_acc = have_acc || acc;
                 __syncwarp();
             }
-            if (err != ERR_NONE) break;
-            // ---- score the pass and keep the selected one ----
-            const double score = fsr_score_warp(bx, bzs, z2s, bis, nb, I.mu,
-                                                reinterpret_cast<char*>(candA), lane, nullptr);
-            const bool acc = !I.has_theta || score >= I.theta;
-            bool take;
-            if (acc) take = !have_acc || vol > best_vol || (vol == best_vol && nb > best_n);
-            else take = !have_acc && (!have_any || vol > best_vol || (vol == best_vol && nb > best_n));
-            if (take) {
-                best_vol = vol;
-                best_n = nb;
-                best_score = score;
-                if (pass_out != best_out)
-                    for (int i = lane; i < nb; i += 32) best_out[i] = pass_out[i];
-            }
-            have_any = true;
-            have_acc = have_acc || acc;
-            __syncwarp();
+            PLP_SYNC()   // FSR scratch overlays the point buffers
         }
-        if (lane == 0) {
+        if (g == 0 && lane == 0) {
             if (err) atomicOr(a.err_flag, 1 << err);
             SlotHead h;
             h.n_boxes = err ? 0 : best_n;
@@ -473,8 +797,19 @@ __global__ void __launch_bounds__(128, 1) decoder_kernel(DecoderArgs a) {
             h.fallback = have_acc ? 0 : 1;
             a.heads[slot] = h;
         }
-        __syncwarp();
+        PLP_SYNC()
     }
+}
+
+template <int G, int D, int M>
+__global__ void __launch_bounds__(32 * G * D, M) decoder_kernel(DecoderArgs a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int dec = (threadIdx.x >> 5) / G;
+    const DecLayout lay = dec_layout(a.P, a.C, a.Hz);
+    if (G > 1 && threadIdx.x % (32 * G) == 0)
+        mbar_init(&reinterpret_cast<DecShared*>(smem_raw + (size_t)dec * lay.bytes + lay.off_sh)->bar, G);
+    __syncthreads();
+    decoder_body<G>(a, smem_raw + (size_t)dec * lay.bytes, dec, blockIdx.x * D + dec);
 }
 
 // ---------------------------------------------------------------------------
@@ -654,7 +989,28 @@ __global__ void gather_best_kernel(const InstDesc* __restrict__ inst, int n_inst
 // ---------------------------------------------------------------------------
 // host launchers (engine.hpp)
 // ---------------------------------------------------------------------------
+// (G warps per decoder, D decoders per CTA, M minimum resident CTAs per SM:
+// a register cap of 65536 / (32 G D M) per thread) instantiations
+#define PLP_DECODER_CONFIGS(X)                                                                 \
+    X(1, 2, 1) X(1, 4, 1) X(1, 4, 4) X(1, 8, 1) X(1, 8, 2) X(2, 1, 1) X(2, 2, 1) X(2, 2, 5)     \
+    X(2, 4, 1) X(2, 4, 3) X(4, 1, 1) X(4, 1, 5) X(4, 1, 6) X(4, 2, 1) X(4, 2, 3) X(4, 4, 1)   \
+    X(8, 1, 1) X(8, 1, 3) X(8, 2, 1)
+
+using DecoderFn = void (*)(DecoderArgs);
+
+static DecoderFn decoder_fn(int G, int D, int M) {
+#define PLP_PICK(g, d, m) \
+    if (G == g && D == d && M == m) return decoder_kernel<g, d, m>;
+    PLP_DECODER_CONFIGS(PLP_PICK)
+#undef PLP_PICK
+    return nullptr;
+}
+
+bool decoder_config_supported(int G, int D, int M) { return decoder_fn(G, D, M) != nullptr; }
+
 cudaError_t launch_decoder(const DecodeLaunch& L, cudaStream_t st) {
+    DecoderFn fn = decoder_fn(L.warps_per_decoder, L.decoders_per_cta, L.min_blocks);
+    if (!fn) return cudaErrorInvalidConfiguration;
     DecoderArgs a;
     a.inst = L.inst;
     a.step_type = L.step_type;
@@ -663,29 +1019,32 @@ cudaError_t launch_decoder(const DecodeLaunch& L, cudaStream_t st) {
     a.n_work = L.n_work;
     a.work_next = L.work_next;
     a.err_flag = L.err_flag;
+    a.abort = L.abort;
     a.heads = L.heads;
     a.places = L.places;
     a.scratch = L.scratch;
     a.mt_init = L.mt_init;
     a.P = L.P;
     a.C = L.C;
-    a.dec_bytes = decoder_smem_bytes(L.P, L.C);
-    a.decoders_per_cta = L.decoders_per_cta;
-    const int smem = a.dec_bytes * L.decoders_per_cta;
-    cudaError_t e = cudaFuncSetAttribute(decoder_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    a.Hz = L.Hz;
+    const int smem = decoder_smem_bytes(L.P, L.C, L.Hz) * L.decoders_per_cta;
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
     e = cudaMemsetAsync(L.work_next, 0, sizeof(int), st);
     if (e != cudaSuccess) return e;
-    decoder_kernel<<<L.ctas, 32 * L.decoders_per_cta, smem, st>>>(a);
+    e = cudaMemsetAsync(L.abort, 0, sizeof(int), st);
+    if (e != cudaSuccess) return e;
+    fn<<<L.ctas, 32 * L.warps_per_decoder * L.decoders_per_cta, smem, st>>>(a);
     return cudaGetLastError();
 }
 
-cudaError_t decoder_occupancy(int P, int C, int decoders_per_cta, int* ctas_per_sm) {
-    const int smem = decoder_smem_bytes(P, C) * decoders_per_cta;
-    cudaError_t e = cudaFuncSetAttribute(decoder_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+cudaError_t decoder_occupancy(int P, int C, int Hz, int G, int D, int M, int* ctas_per_sm) {
+    DecoderFn fn = decoder_fn(G, D, M);
+    if (!fn) return cudaErrorInvalidConfiguration;
+    const int smem = decoder_smem_bytes(P, C, Hz) * D;
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas_per_sm, decoder_kernel,
-                                                         32 * decoders_per_cta, smem);
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas_per_sm, fn, 32 * G * D, smem);
 }
 
 cudaError_t launch_select_best(const InstDesc* inst, int n_inst, const SlotHead* heads, int2* best,

@@ -57,6 +57,7 @@ enum DecodeErr : int {
     ERR_BOX_CAP = 1,     // more placed boxes than the shared-memory tile holds
     ERR_CAND_CAP = 2,    // more live extreme points than the tile holds
     ERR_RNG = 3,         // randrange rejection loop exceeded its bound
+    ERR_SYNC = 4,        // a decoder's warps stopped meeting at a barrier (wait bound hit)
 };
 
 // placement word: x | y << 16 | z << 32 | orientation << 48 | type << 51

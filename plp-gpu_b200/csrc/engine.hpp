@@ -15,17 +15,22 @@ struct DecodeLaunch {
     int n_work;
     int* work_next;
     int* err_flag;            // OR of (1 << err) over restarts that failed
+    int* abort;               // set when a bounded barrier wait gives up
     SlotHead* heads;
     unsigned long long* places;
     unsigned long long* scratch;
     const uint32_t* mt_init;
     int P, C;                 // shared-memory tile: boxes and live points per decoder
-    int decoders_per_cta;     // warps (decoders) per CTA, <= 8
+    int Hz;                   // entries of the top-z index (max height + 2), 0 = none
+    int warps_per_decoder;    // G
+    int decoders_per_cta;     // D
+    int min_blocks;           // M (register cap through the launch bounds)
     int ctas;
 };
 
-int decoder_smem_bytes(int P, int C);
-cudaError_t decoder_occupancy(int P, int C, int decoders_per_cta, int* ctas_per_sm);
+int decoder_smem_bytes(int P, int C, int Hz);
+bool decoder_config_supported(int G, int D, int M);
+cudaError_t decoder_occupancy(int P, int C, int Hz, int G, int D, int M, int* ctas_per_sm);
 cudaError_t launch_decoder(const DecodeLaunch& L, cudaStream_t st);
 cudaError_t launch_select_best(const InstDesc* inst, int n_inst, const SlotHead* heads, int2* best,
                                cudaStream_t st);

@@ -99,7 +99,7 @@ def lib():
         "plp_run_plain": (ctypes.c_int, [P, P, P]),
         "plp_create": (ctypes.c_int, [SZ, I32, P]),
         "plp_destroy": (None, [P]),
-        "plp_set_tile": (ctypes.c_int, [P, I32, I32, I32]),
+        "plp_set_tile": (ctypes.c_int, [P, I32, I32, I32, I32, I32]),
         "plp_solve": (ctypes.c_int, [P, P, I32, P, I32, P]),
         "plp_submit": (ctypes.c_int, [P, P, P, P]),
         "plp_poll": (ctypes.c_int, [P, I64]),
@@ -322,8 +322,8 @@ class Handle:
     def __exit__(self, *exc):
         self.close()
 
-    def set_tile(self, P: int, C: int, D: int):
-        _check(lib().plp_set_tile(self._p, P, C, D), self._p)
+    def set_tile(self, P: int = 0, C: int = 0, G: int = 0, D: int = 0, M: int = 0):
+        _check(lib().plp_set_tile(self._p, P, C, G, D, M), self._p)
 
     def solve(self, instances, opts) -> list:
         """opts: one RunOpts for all instances or a list with one per instance."""

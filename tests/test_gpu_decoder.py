@@ -71,7 +71,7 @@ def test_solve_tiny_tile_retries_give_same_results(handle):
     text = synth.stress(40003).to_thpack()
     inst = P.Instance.parse(text)
     h2 = P.Handle()
-    h2.set_tile(16, 32, 4)
+    h2.set_tile(P=16, C=32, G=1, D=4)
     r_small = h2.solve([inst], P.make_opts(seed=7, restarts=8))[0]
     h2.close()
     r_ref = handle.solve([inst], P.make_opts(seed=7, restarts=8))[0]
@@ -106,3 +106,25 @@ def test_plain_path_matches_oracle(kw):
     for k in range(2):
         js, _, _ = O.run(oi, seed=4 + k, passes=passes, **kw)
         assert O.strip_time(r.json(k)) == O.strip_time(js)
+
+
+CONFIGS = [(1, 2, 1), (1, 4, 1), (1, 4, 4), (1, 8, 1), (1, 8, 2), (2, 1, 1), (2, 2, 1), (2, 2, 5), (2, 4, 1),
+           (2, 4, 3), (4, 1, 1), (4, 1, 5), (4, 1, 6), (4, 2, 1), (4, 2, 3), (4, 4, 1), (8, 1, 1), (8, 1, 3),
+           (8, 2, 1)]
+
+
+@pytest.mark.parametrize("G,D,M", CONFIGS)
+def test_every_tile_config_matches_oracle(G, D, M):
+    """Warps per decoder and decoders per CTA change speed only."""
+    texts = [synth.single_pass(1).to_thpack(), synth.stress(40002).to_thpack(),
+             synth.batched(30009).to_thpack()]
+    insts = [P.Instance.parse(t) for t in texts]
+    with P.Handle() as h:
+        h.set_tile(P=64, C=128, G=G, D=D, M=M)   # shallow: some restarts also take the retry path
+        res = h.solve(insts, [P.make_opts(seed=0, restarts=4, eps=0.0, theta=None),
+                              P.make_opts(seed=5, restarts=4), P.make_opts(seed=9, restarts=4, passes=2)])
+    for t, r, (seed, kw) in zip(texts, res, [(0, dict(eps=0.0, theta=None)), (5, {}), (9, dict(passes=2))]):
+        oi = O.OInstance(t)
+        for k in range(4):
+            js, _, _ = O.run(oi, seed=seed + k, **kw)
+            assert O.strip_time(r.json(k)) == O.strip_time(js), (G, D, M, seed + k)
