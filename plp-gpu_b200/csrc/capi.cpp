@@ -91,7 +91,7 @@ struct TileConfig {
     int P = 128;       // placed-box tile depth per decoder
     int C = 384;       // live-point tile depth per decoder
     int G = 1;         // warps per decoder
-    int D = 4;         // decoders per CTA
+    int D = 8;         // decoders per CTA
     int M = 1;         // minimum resident CTAs per SM (register cap)
 };
 

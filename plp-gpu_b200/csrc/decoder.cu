@@ -396,16 +396,16 @@ __device__ __forceinline__ void scan_points(DecShared* sh, const uint2* W, unsig
                                 b.y < y + S.dmax && bz[u] < z + S.hmax;
                 near |= (nu ? 1u : 0u) << u;
             }
-            unsigned todo = __reduce_or_sync(FULL, near);
-            while (todo) {
-                const int u = __ffs(todo) - 1;
-                todo &= todo - 1;
-                if ((near >> u) & 1u) {
-                    const int4 b = bb[u];
-                    const int bzu = bz[u];
+            const unsigned todo = __reduce_or_sync(FULL, near);
 #pragma unroll
-                    for (int o = 0; o < 6; o++)
-                        if (b.x < x + S.ow[o] && b.y < y + S.od[o] && bzu < z + S.oh[o]) alive &= ~(1u << o);
+            for (int u = 0; u < 4; u++) {
+                if ((todo >> u) & 1u) {                 // uniform: some lane is near box u
+                    if ((near >> u) & 1u) {
+                        const int4 b = bb[u];
+#pragma unroll
+                        for (int o = 0; o < 6; o++)
+                            if (b.x < x + S.ow[o] && b.y < y + S.od[o] && bz[u] < z + S.oh[o]) alive &= ~(1u << o);
+                    }
                 }
             }
             if (!__any_sync(FULL, alive != 0)) break;
