@@ -206,6 +206,31 @@ int plp_cancel(plp_handle* h, int64_t request_id);
 int plp_request_times(plp_handle* h, int64_t request_id, double* queued_s, double* total_s);
 
 /* ------------------------------------------------------------------------ */
+/* allocation-free decode                                                    */
+/* ------------------------------------------------------------------------ */
+/* No counterpart in the reference. For callers that cannot allocate device
+ * memory -- a process whose device memory is owned by another framework's
+ * caching allocator, a plugin hosted by a runtime that forbids allocation on
+ * its request path, a latency-critical loop that must not enter the
+ * allocator: decodes every restart of one instance like plp_solve, but the
+ * decoder's scratch (tables, work list, counters, multi-pass rows) is a fixed
+ * 8 MiB array inside the library, so the call allocates no device memory.
+ *   d_heads:  opts->restarts records of 32 bytes {int32 n_boxes, int32 err,
+ *             int64 volume, double score, int32 n_passes, int32 fallback}
+ *   d_places: opts->restarts rows of max(n_items, 1) uint64 words, placement i
+ *             = x | y << 16 | z << 32 | orientation index << 48 | type << 51
+ * Both are caller-owned device buffers. The work is enqueued on `stream`
+ * (a cudaStream_t, NULL = legacy default stream); synchronise it before
+ * reading the outputs. The first call on each device looks up the scratch's
+ * device address (cudaGetSymbolAddress); make that first call before any
+ * stream capture. Every call shares the scratch, so calls that overlap on the
+ * GPU race: serialise them (one stream, or wait between calls). Instances
+ * whose tables do not fit the scratch (about 8 MiB of restarts x 8 bytes,
+ * types x 88 bytes and steps x 4 bytes) return PLP_E_CAPACITY. */
+int plp_decode_noalloc(const plp_instance* inst, const plp_run_opts* opts, void* d_heads,
+                       void* d_places, void* stream);
+
+/* ------------------------------------------------------------------------ */
 /* kernel-level hooks (parity tests of the individual device kernels)        */
 /* ------------------------------------------------------------------------ */
 /* device MT19937 (kernel c): for each seed, n_random random() doubles then

@@ -262,8 +262,9 @@ struct Pinned {
 
 }  // namespace
 
-// gather of the best restart's placements (decoder.cu)
+// gather of the best restart's placements (decoder.cu); fixed scratch (noalloc.cu)
 namespace plpb {
+cudaError_t noalloc_scratch(void** ptr, size_t* bytes);
 cudaError_t launch_gather_best(const InstDesc* inst, int n_inst, const int2* best,
                                const unsigned long long* places, unsigned long long* out,
                                int out_stride, cudaStream_t st);
@@ -1288,6 +1289,91 @@ void plp_batch_free(plp_batch* pb) {
         batch_release(pb->b, pb->h->sync_stream);
     }
     delete pb;
+}
+
+// ---- allocation-free decode --------------------------------------------------
+int plp_decode_noalloc(const plp_instance* inst, const plp_run_opts* opts, void* d_heads,
+                       void* d_places, void* stream) {
+    if (!inst || !opts || !d_heads || !d_places)
+        return set_error(PLP_E_INVALID, "plp_decode_noalloc: null argument");
+    if (opts->restarts < 1 || opts->passes < 1 || (opts->order != 0 && opts->order != 1))
+        return set_error(PLP_E_INVALID, "plp_decode_noalloc: bad options");
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    Batch b;
+    int s = b.build({&inst->inst}, {*opts});
+    if (s != PLP_OK) return s;
+    // Tile deep enough that no restart can outgrow it: every placement adds
+    // at most 7 live points (its 8 corners minus the one it covers), and at
+    // most one box is placed per step.
+    const int steps = std::max(1, b.desc[0].n_steps);
+    TileConfig t;
+    t.P = (steps + 15) & ~15;
+    t.C = std::min(C_MAX, ((1 + 7 * steps) + 31) & ~31);
+    t.G = 1;
+    t.M = 1;
+    t.D = 8;
+    while (t.D > 2 && decoder_smem_bytes(t.P, t.C, b.Hz) * t.D > 200 * 1024) t.D >>= 1;
+    if (t.P > P_MAX || decoder_smem_bytes(t.P, t.C, b.Hz) * t.D > 227 * 1024 || 1 + 7 * steps > C_MAX)
+        return set_error(PLP_E_CAPACITY, "plp_decode_noalloc: instance too large for the shared-memory tile");
+    // scratch: the address is set up on the first call on each device
+    void* scr = nullptr;
+    size_t cap = 0;
+    cudaError_t e = noalloc_scratch(&scr, &cap);
+    if (e != cudaSuccess) return set_cuda_error("plp_decode_noalloc: scratch address", e);
+    int dev = 0, sms = 148, occ = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    e = decoder_occupancy(t.P, t.C, b.Hz, t.G, t.D, t.M, &occ);
+    if (e != cudaSuccess) return set_cuda_error("plp_decode_noalloc: occupancy", e);
+    occ = std::max(occ, 1);
+    long long ctas = std::max<long long>(1, std::min<long long>((b.n_slots + t.D - 1) / t.D, (long long)sms * occ));
+    auto al = [](size_t v) { return (v + 255) & ~size_t(255); };
+    const size_t o_mt = 0;
+    const size_t o_desc = al(o_mt + 624 * 4);
+    const size_t o_steps = al(o_desc + sizeof(InstDesc));
+    const size_t o_types = al(o_steps + std::max<size_t>(1, b.steps.size()) * sizeof(int));
+    const size_t o_work = al(o_types + std::max<size_t>(1, b.types.size()) * sizeof(TypeOrs));
+    const size_t o_flags = al(o_work + b.work.size() * sizeof(int2));
+    const size_t o_rows = al(o_flags + 16);
+    const size_t row_bytes = (size_t)t.D * b.max_stride * 8;   // multi-pass rows of one CTA
+    if (o_rows > cap || (b.multi_pass && o_rows + row_bytes > cap))
+        return set_error(PLP_E_CAPACITY, "plp_decode_noalloc: tables exceed the 8 MiB fixed scratch "
+                                         "(fewer restarts, steps or types per call)");
+    if (b.multi_pass) ctas = std::min<long long>(ctas, (long long)((cap - o_rows) / row_bytes));
+    // tables staged in host memory and copied in one transfer; the counters
+    // and flags that must start at zero are zero in the staged bytes
+    std::vector<unsigned char> host(o_rows, 0);
+    mt_init_table(reinterpret_cast<uint32_t*>(host.data() + o_mt));
+    std::memcpy(host.data() + o_desc, b.desc.data(), sizeof(InstDesc));
+    std::memcpy(host.data() + o_steps, b.steps.data(), b.steps.size() * sizeof(int));
+    std::memcpy(host.data() + o_types, b.types.data(), b.types.size() * sizeof(TypeOrs));
+    std::memcpy(host.data() + o_work, b.work.data(), b.work.size() * sizeof(int2));
+    char* d = static_cast<char*>(scr);
+    e = cudaMemcpyAsync(d, host.data(), host.size(), cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return set_cuda_error("plp_decode_noalloc: table copy", e);
+    DecodeLaunch L{};
+    L.inst = reinterpret_cast<const InstDesc*>(d + o_desc);
+    L.step_type = reinterpret_cast<const int*>(d + o_steps);
+    L.types = reinterpret_cast<const TypeOrs*>(d + o_types);
+    L.work = reinterpret_cast<const int2*>(d + o_work);
+    L.n_work = (int)b.work.size();
+    L.work_next = reinterpret_cast<int*>(d + o_flags);
+    L.err_flag = reinterpret_cast<int*>(d + o_flags + 8);
+    L.abort = reinterpret_cast<int*>(d + o_flags + 12);
+    L.heads = static_cast<SlotHead*>(d_heads);
+    L.places = static_cast<unsigned long long*>(d_places);
+    L.scratch = reinterpret_cast<unsigned long long*>(d + o_rows);
+    L.mt_init = reinterpret_cast<const uint32_t*>(d + o_mt);
+    L.P = t.P;
+    L.C = t.C;
+    L.Hz = b.Hz;
+    L.warps_per_decoder = t.G;
+    L.decoders_per_cta = t.D;
+    L.min_blocks = t.M;
+    L.ctas = (int)ctas;
+    e = launch_decoder(L, st);
+    if (e != cudaSuccess) return set_cuda_error("plp_decode_noalloc: decoder launch", e);
+    return PLP_OK;
 }
 
 // ---- reference work accounting ---------------------------------------------

@@ -113,6 +113,7 @@ def lib():
         "plp_batch_io_bytes": (ctypes.c_int, [P, P, P]),
         "plp_batch_free": (None, [P]),
         "plp_result_work": (ctypes.c_int, [P, I32, P, P]),
+        "plp_decode_noalloc": (ctypes.c_int, [P, P, P, P, P]),
         "plp_rng_dump": (ctypes.c_int, [P, I32, I32, I32, I32, P, P]),
         "plp_rng_dump_host": (ctypes.c_int, [P, I32, I32, I32, I32, P, P]),
         "plp_fsr_score": (ctypes.c_int, [P, P, I32, D, P, P]),
