@@ -209,6 +209,48 @@ def run_reference(args):
     return 0
 
 
+def serving_report(device: int, rates=(100, 1000, 10000), window_s=2.0, max_requests=600):
+    """Poisson streams of pallet-solve requests (batched-workload sizes,
+    restarts drawn from {64, 256, 1024}) through the serving loop; p50/p99
+    latency from submit to result, and the sustained solve rate. The plain
+    comparison solves the same requests one at a time (one plp_solve each,
+    no batching), back to back."""
+    out = []
+    for rate in rates:
+        n = int(min(max_requests, max(20, rate * window_s)))
+        stream = synth.serving_stream(n, float(rate), seed=50000 + rate)
+        insts = [P.Instance.parse(i.to_thpack()) for _, i, _ in stream]
+        opts = [P.make_opts(seed=k, restarts=r) for k, (_, _, r) in enumerate(stream)]
+        with P.Handle(device=device) as h:
+            h.solve([insts[0]], opts[0])                 # warm the pool and kernels
+            t0 = time.perf_counter()
+            ids = []
+            for (arrive, _, _), inst, o in zip(stream, insts, opts):
+                delay = arrive - (time.perf_counter() - t0)
+                if delay > 0:
+                    time.sleep(delay)
+                ids.append(h.submit(inst, o))
+            lat = []
+            for rid in ids:
+                if h.wait(rid, 600000) != P.OK:
+                    raise SystemExit(f"serving request failed: {P.last_error()}")
+                lat.append(h.times(rid)[1])
+                h.take(rid)
+            span = time.perf_counter() - t0
+            # plain: the same requests solved one by one
+            t1 = time.perf_counter()
+            for inst, o in zip(insts[:min(n, 100)], opts[:min(n, 100)]):
+                h.solve([inst], o)
+            plain_per = (time.perf_counter() - t1) / min(n, 100)
+        lat.sort()
+        q = lambda p: 1000 * lat[min(len(lat) - 1, int(p * len(lat)))]
+        out.append({"rate_per_s": rate, "requests": n, "p50_ms": q(0.50), "p99_ms": q(0.99),
+                    "solves_per_s": n / span,
+                    "decodes_per_s": sum(o.restarts for o in opts) / span,
+                    "plain_solve_ms": 1000 * plain_per})
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -219,6 +261,7 @@ def main():
                     choices=["multi_restart", "batched", "stress", "single_pass"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-serving", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -335,6 +378,7 @@ def main():
             plain = {"value": pv, "unit": "decodes/s", "sample": f"{n_pl} restarts, one device "
                      "feasibility launch per item step (plp_run_plain)", "speedup_of_persistent": value / world / pv}
             del o_pl
+        serving = None if args.no_serving else serving_report(local)
         out = {
             "metric": "decodes/sec", "value": value, "unit": "decodes/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
@@ -352,6 +396,7 @@ def main():
             "roofline": roofline,
             "cpu_baseline": cpu,
             "plain_path": plain,
+            "serving": serving,
             "clocks": clk,
         }
         print(json.dumps(out))

@@ -128,3 +128,17 @@ def test_every_tile_config_matches_oracle(G, D, M):
         for k in range(4):
             js, _, _ = O.run(oi, seed=seed + k, **kw)
             assert O.strip_time(r.json(k)) == O.strip_time(js), (G, D, M, seed + k)
+
+
+def test_reference_work_accounting_matches_oracle_counter(handle):
+    """plp_result_work replays the reference candidate list: T equals the
+    oracle's instrumented count of AABB tests (the roofline's unit)."""
+    for make, seeds in ((lambda: synth.multi_restart(2), 6), (lambda: synth.stress(40006), 3),
+                        (lambda: synth.single_pass(1), 2)):
+        text = make().to_thpack()
+        inst = P.Instance.parse(text)
+        r = handle.solve([inst], P.make_opts(seed=11, restarts=seeds))[0]
+        oi = O.OInstance(text)
+        for k in range(seeds):
+            _, _, _, st = O.run(oi, seed=11 + k, stats=True)
+            assert r.work(k) == (st["aabb_full"], st["pairs"])

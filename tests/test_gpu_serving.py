@@ -1,0 +1,79 @@
+"""Serving loop: continuous batching of requests admitted by a device-memory
+budget. Each request's result must be identical alone and in the mix (bit
+for bit: every restart's JSON without time_s)."""
+import random
+import time
+
+import pytest
+
+import oracle_py as O
+import plpb200 as P
+from plpb200 import synth
+
+pytestmark = pytest.mark.gpu
+
+
+def _requests(n, seed=5):
+    rng = random.Random(seed)
+    out = []
+    for i in range(n):
+        inst = synth.batched(60000 + i)
+        out.append((inst.to_thpack(), P.make_opts(seed=rng.randrange(1000), restarts=rng.choice((4, 16, 64)),
+                                                   eps=rng.choice((0.0, 0.3)))))
+    return out
+
+
+def _jsons(res):
+    return [O.strip_time(res.json(k)) for k in range(res.restarts)]
+
+
+def test_results_identical_alone_and_in_the_mix():
+    reqs = _requests(24)
+    insts = [P.Instance.parse(t) for t, _ in reqs]
+    with P.Handle() as h:
+        alone = [_jsons(h.solve([i], o)[0]) for i, (_, o) in zip(insts, reqs)]
+        ids = []
+        for i, (_, o) in zip(insts, reqs):
+            ids.append(h.submit(i, o))
+            time.sleep(0.0005)                      # staggered arrivals join running waves
+        for rid in ids:
+            assert h.wait(rid, 120000) == P.OK, P.last_error()
+        mixed = [_jsons(h.take(rid)) for rid in ids]
+    assert mixed == alone
+
+
+def test_small_budget_serialises_but_stays_exact():
+    reqs = _requests(6, seed=9)
+    insts = [P.Instance.parse(t) for t, _ in reqs]
+    with P.Handle() as h:
+        alone = [_jsons(h.solve([i], o)[0]) for i, (_, o) in zip(insts, reqs)]
+    with P.Handle(budget_bytes=4 << 20) as h:      # about one request at a time
+        ids = [h.submit(i, o) for i, (_, o) in zip(insts, reqs)]
+        for rid in ids:
+            assert h.wait(rid, 120000) == P.OK
+        assert [_jsons(h.take(rid)) for rid in ids] == alone
+
+
+def test_over_budget_request_is_refused():
+    inst = P.Instance.parse(synth.multi_restart(2).to_thpack())
+    with P.Handle(budget_bytes=64 << 10) as h:
+        with pytest.raises(P.PlpError) as e:
+            h.submit(inst, P.make_opts(restarts=1024))
+        assert e.value.status == P.E_BUDGET
+
+
+def test_cancel_and_timeouts():
+    reqs = _requests(12, seed=3)
+    insts = [P.Instance.parse(t) for t, _ in reqs]
+    with P.Handle(budget_bytes=2 << 20) as h:      # forces a queue
+        ids = [h.submit(i, P.make_opts(seed=1, restarts=64)) for i in insts]
+        h.cancel(ids[-1])
+        statuses = [h.wait(rid, 120000) for rid in ids]
+        assert statuses[-1] in (P.E_CANCELLED, P.OK)   # it may already have been running
+        assert all(s == P.OK for s in statuses[:-1])
+        q, t = h.times(ids[0])
+        assert t >= q >= 0
+        with pytest.raises(P.PlpError) as e:
+            h.take(10 ** 9)
+        assert e.value.status == P.E_NOT_FOUND
+        assert h.poll(10 ** 9) == P.E_NOT_FOUND
