@@ -100,8 +100,16 @@ struct TileConfig {
 void remember_tile(TileConfig& keep, const TileConfig& used) {
     keep.P = std::max(keep.P, used.P);
     keep.C = std::max(keep.C, used.C);
-    while (keep.D > 1 && decoder_smem_bytes(keep.P, keep.C, 4096) * keep.D > 200 * 1024) keep.D >>= 1;
+    while (keep.D > 1 && decoder_smem_bytes(keep.P, keep.C, 0, keep.G) * keep.D > 200 * 1024) keep.D >>= 1;
     if (!decoder_config_supported(keep.G, keep.D, keep.M)) keep.M = 1;
+}
+
+// Fewer decoders per CTA when the tile plus this batch's top-z index (Hz
+// entries) would not fit one CTA's shared memory.
+void fit_tile(TileConfig& t, int Hz) {
+    while (t.D > 1 && decoder_smem_bytes(t.P, t.C, Hz, t.G) * t.D > 227 * 1024) t.D >>= 1;
+    while (!decoder_config_supported(t.G, t.D, t.M) && t.D > 1) t.D >>= 1;
+    if (!decoder_config_supported(t.G, t.D, t.M)) t.M = 1;
 }
 
 constexpr int P_MAX = 2048;
@@ -373,6 +381,7 @@ int batch_execute(Batch& b, cudaStream_t st, int sms, TileConfig& tile, ExecStat
     };
     ExecStats x;
     TileConfig t = tile;
+    fit_tile(t, b.Hz);
     const int2* d_work = reinterpret_cast<const int2*>(b.d_mem + b.o_work);
     int* d_flag = reinterpret_cast<int*>(b.d_mem + b.o_next + 8);
     cudaError_t e = cudaMemsetAsync(d_flag, 0, 8, st);
@@ -418,10 +427,10 @@ int batch_execute(Batch& b, cudaStream_t st, int sms, TileConfig& tile, ExecStat
         if (grow_p) t.P = std::min(P_MAX, std::max(t.P * 2, 32));
         if (grow_c) t.C = std::min(C_MAX, t.C * 2);
         // deeper tiles: fewer decoders per CTA keeps one CTA within 227 KB
-        while (t.D > 1 && decoder_smem_bytes(t.P, t.C, b.Hz) * t.D > 200 * 1024) t.D >>= 1;
+        while (t.D > 1 && decoder_smem_bytes(t.P, t.C, b.Hz, t.G) * t.D > 200 * 1024) t.D >>= 1;
         while (!decoder_config_supported(t.G, t.D, t.M) && t.D > 1) t.D >>= 1;
         if (!decoder_config_supported(t.G, t.D, t.M)) t.M = 1;
-        if (decoder_smem_bytes(t.P, t.C, b.Hz) > 227 * 1024 || !decoder_config_supported(t.G, t.D, t.M)) {
+        if (decoder_smem_bytes(t.P, t.C, b.Hz, t.G) > 227 * 1024 || !decoder_config_supported(t.G, t.D, t.M)) {
             batch_release(b, st);
             return set_error(PLP_E_CAPACITY, "instance needs a larger tile than shared memory holds");
         }
@@ -1009,7 +1018,7 @@ int plp_set_tile(plp_handle* h, int32_t P, int32_t C, int32_t G, int32_t D, int3
         record(h, s);
         return s;
     }
-    if (decoder_smem_bytes(t.P, t.C, 4096) * t.D > 227 * 1024) {
+    if (decoder_smem_bytes(t.P, t.C, 0, t.G) * t.D > 227 * 1024) {   // a batch's z index may lower D
         int s = set_error(PLP_E_CAPACITY, "plp_set_tile: tile exceeds shared memory");
         record(h, s);
         return s;
@@ -1312,8 +1321,8 @@ int plp_decode_noalloc(const plp_instance* inst, const plp_run_opts* opts, void*
     t.G = 1;
     t.M = 1;
     t.D = 8;
-    while (t.D > 2 && decoder_smem_bytes(t.P, t.C, b.Hz) * t.D > 200 * 1024) t.D >>= 1;
-    if (t.P > P_MAX || decoder_smem_bytes(t.P, t.C, b.Hz) * t.D > 227 * 1024 || 1 + 7 * steps > C_MAX)
+    while (t.D > 2 && decoder_smem_bytes(t.P, t.C, b.Hz, t.G) * t.D > 200 * 1024) t.D >>= 1;
+    if (t.P > P_MAX || decoder_smem_bytes(t.P, t.C, b.Hz, t.G) * t.D > 227 * 1024 || 1 + 7 * steps > C_MAX)
         return set_error(PLP_E_CAPACITY, "plp_decode_noalloc: instance too large for the shared-memory tile");
     // scratch: the address is set up on the first call on each device
     void* scr = nullptr;

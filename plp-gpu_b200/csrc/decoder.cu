@@ -98,7 +98,42 @@ __host__ __device__ inline DecLayout dec_layout(int P, int C, int Hz) {
     return l;
 }
 
-int decoder_smem_bytes(int P, int C, int Hz) { return dec_layout(P, C, Hz).bytes; }
+// Layout of one single-warp (incremental) decoder: as above, but every live
+// point also carries its evaluation state and six contact areas.
+struct Dec1Layout {
+    int off_bx, off_bz, off_z2, off_bi, off_key, off_st, off_sup, off_w, off_wi, off_zt, off_sh, bytes;
+};
+
+__host__ __device__ inline Dec1Layout dec1_layout(int P, int C, int Hz) {
+    Dec1Layout l;
+    int o = 624 * 4;                       // MT state
+    o = (o + 15) & ~15;
+    l.off_bx = o;  o += 16 * P;            // int4 {x, y, x2, y2}
+    l.off_bz = o;  o += 4 * P;             // bottom z
+    l.off_z2 = o;  o += 4 * P;             // top z
+    l.off_bi = o;  o += 2 * P;             // placement index
+    o = (o + 15) & ~15;
+    // live points: key, state, 6 contact areas; FSR overlays 18 bytes per box
+    l.off_key = o;
+    l.off_st = o + 4 * C;
+    l.off_sup = o + 8 * C;
+    int region = 32 * C;
+    if (region < 18 * P + 32) region = 18 * P + 32;
+    o += region;
+    o = (o + 15) & ~15;
+    l.off_w = o;   o += 8 * C;             // items to evaluate {key, m2 | jlo << 8 | jsup << 20}
+    l.off_wi = o;  o += 2 * C;             // their point index
+    o = (o + 15) & ~15;
+    l.off_zt = o;  o += 2 * Hz;            // u16: boxes with top < z
+    o = (o + 15) & ~15;
+    l.off_sh = o;  o += (int)sizeof(DecShared);
+    l.bytes = o;
+    return l;
+}
+
+int decoder_smem_bytes(int P, int C, int Hz, int G) {
+    return G == 1 ? dec1_layout(P, C, Hz).bytes : dec_layout(P, C, Hz).bytes;
+}
 
 struct DecoderArgs {
     const InstDesc* __restrict__ inst;
@@ -237,7 +272,7 @@ __device__ __forceinline__ double fsr_score_warp(const int4* bx, const int* bz, 
 // if it gives up, or another warp of the launch already gave up, the
 // launch-wide abort flag is set and the caller unwinds, so a broken
 // synchronisation ends the launch with ERR_SYNC instead of hanging the GPU.
-constexpr int SYNC_WAIT_LIMIT = 1 << 20;
+constexpr int SYNC_WAIT_LIMIT = 1 << 18;   // tries of up to ~10 us each: bounded near 3 s
 
 __device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
     const unsigned a = (unsigned)__cvta_generic_to_shared(bar);
@@ -249,15 +284,17 @@ __device__ __forceinline__ void mbar_arrive(unsigned long long* bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(a) : "memory");
 }
 
+// The waiting thread may be suspended until the phase completes or about
+// 10 us pass (suspend-time hint), so waiting warps do not spin on issue slots.
 __device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
     const unsigned a = (unsigned)__cvta_generic_to_shared(bar);
     unsigned ok;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
         "selp.u32 %0, 1, 0, p;\n\t}"
         : "=r"(ok)
-        : "r"(a), "r"(parity)
+        : "r"(a), "r"(parity), "r"(10000u)
         : "memory");
     return ok != 0;
 }
@@ -274,7 +311,7 @@ struct GroupSync {
         if (lane == 0) mbar_arrive(bar);
         bool ok = true;
         for (int k = 0; !mbar_try_wait(bar, phase); k++) {
-            if (k >= SYNC_WAIT_LIMIT || *reinterpret_cast<volatile int*>(abort)) {
+            if (k >= SYNC_WAIT_LIMIT || ((k & 63) == 63 && *reinterpret_cast<volatile int*>(abort))) {
                 ok = false;
                 break;
             }
@@ -813,6 +850,600 @@ __global__ void __launch_bounds__(32 * G * D, M) decoder_kernel(DecoderArgs a) {
 }
 
 // ---------------------------------------------------------------------------
+// incremental single-warp decoder (G = 1)
+// ---------------------------------------------------------------------------
+// Every live point carries its evaluation for the current item type:
+//   st bits 0-5   C2 mask m2 (orientation inside the container)
+//   st bits 8-13  C1 blocked orientations (exact for the bits of `known`)
+//   st bits 16-21 C3 support-ok orientations (all six at z = 0)
+//   st bits 24-29 known = m2 & support-ok when C1 was evaluated
+//   st bit  31    valid
+//   sup[o]        integer contact area under orientation o (z > 0)
+// Boxes are only ever added during a pass, so a blocked orientation stays
+// blocked and a contact area only grows: a valid point stays exact if each
+// newly placed box is applied to it once (C1 OR, C3 sum), which the next
+// step's filter pass does. Consecutive items of the same type share the
+// evaluation; a type change invalidates every point. A point is evaluated
+// from scratch (all boxes) only while it is invalid: new corners, points the
+// greedy scan has not reached yet, and points whose support grew onto an
+// orientation whose C1 was never evaluated.
+//
+// The C3 test is the integer form of the reference's FP64 ratio:
+// (double)s / (double)(w*d) < 0.5  <=>  2 s < w d. Both s and w d are
+// integers below 2^52, so both doubles are exact; if s/(wd) < 1/2 then
+// s/(wd) <= 1/2 - 1/(2wd) <= 1/2 - 2^-53, a double below 1/2 that bounds the
+// rounded quotient from above (rounding is monotone); if s/(wd) >= 1/2 the
+// rounded quotient is >= 1/2 as well.
+constexpr uint32_t ST_VALID = 1u << 31;
+
+__device__ __forceinline__ uint32_t st_pack(unsigned m2, unsigned blk, unsigned sok, unsigned known) {
+    return ST_VALID | m2 | (blk << 8) | (sok << 16) | (known << 24);
+}
+__device__ __forceinline__ unsigned st_feasible(uint32_t s) {
+    return (s & ST_VALID) ? (s & (s >> 16) & ~(s >> 8) & 0x3fu) : 0u;
+}
+
+// Evaluates items W[w0 .. w1) from scratch and stores their state. A group
+// of 2^lg lanes shares one item (lanes take every 2^lg-th box), 32 >> lg
+// items at a time, lg chosen so that a short item list still spreads over the
+// whole warp. Greedy mode stops after the first group holding a feasible
+// item. Returns {first feasible item or INT_MAX, end of the evaluated range}.
+template <bool GREEDY>
+__device__ __forceinline__ int2 eval_items(const uint2* W, const unsigned short* wi, int w0, int w1,
+                                           const int4* bx, const int* bzs, int nb, const StepOrs& S,
+                                           uint32_t xmask, uint32_t ymask, int xb, int xyb,
+                                           uint32_t* st, int* sup, int C, int lane) {
+    int first = INT_MAX;
+    int w = w0;
+    while (w < w1) {
+        const int K = min(32, w1 - w);
+        const int lg = K > 16 ? 0 : K > 8 ? 1 : K > 4 ? 2 : K > 2 ? 3 : K > 1 ? 4 : 5;
+        const int span = 1 << lg;
+        const int q = lane >> lg, ph = lane & (span - 1);
+        const bool has = q < K;
+        const uint2 e = has ? W[w + q] : make_uint2(0, 0);
+        const unsigned m2 = e.y & 0x3fu;
+        const int jlo = (int)((e.y >> 8) & 0xfffu), jsup = (int)(e.y >> 20);
+        const int x = (int)(e.x & xmask), y = (int)((e.x >> xb) & ymask), z = (int)(e.x >> xyb);
+        const bool supz = has && z > 0;
+        int a0 = 0, a1 = 0, a2 = 0, a3 = 0, a4 = 0, a5 = 0;
+        // C3: boxes whose top is z
+        const int slo = __reduce_min_sync(FULL, supz ? jlo : INT_MAX);
+        const int shi = __reduce_max_sync(FULL, supz ? jsup : 0);
+        for (int j0 = slo; j0 < shi; j0 += 4 << lg) {
+            int4 bb[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const int j = j0 + (u << lg) + ph;
+                bb[u] = j < shi ? bx[j] : make_int4(0, 0, 0, 0);
+            }
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const int j = j0 + (u << lg) + ph;
+                const int4 b = bb[u];
+                if (supz && j >= jlo && j < jsup) {
+#define PLP_ACC(o, av)                                                   \
+    {                                                                    \
+        const int ox = min(x + S.ow[o], b.z) - max(x, b.x);              \
+        const int oy = min(y + S.od[o], b.w) - max(y, b.y);              \
+        if (ox > 0 && oy > 0) av += ox * oy;                             \
+    }
+                    PLP_ACC(0, a0) PLP_ACC(1, a1) PLP_ACC(2, a2) PLP_ACC(3, a3) PLP_ACC(4, a4) PLP_ACC(5, a5)
+#undef PLP_ACC
+                }
+            }
+        }
+        for (int m = 1; m < span; m <<= 1) {
+            a0 += __shfl_xor_sync(FULL, a0, m);
+            a1 += __shfl_xor_sync(FULL, a1, m);
+            a2 += __shfl_xor_sync(FULL, a2, m);
+            a3 += __shfl_xor_sync(FULL, a3, m);
+            a4 += __shfl_xor_sync(FULL, a4, m);
+            a5 += __shfl_xor_sync(FULL, a5, m);
+        }
+        unsigned sok = 0x3fu;
+        if (z > 0) {
+            const int av[6] = {a0, a1, a2, a3, a4, a5};
+            sok = 0;
+#pragma unroll
+            for (int o = 0; o < 6; o++)
+                if (2LL * av[o] >= (long long)S.wd[o]) sok |= 1u << o;
+        }
+        const unsigned known = m2 & sok;
+        unsigned alive = has ? known : 0u;
+        // C1: boxes above z, 4 per lane per round; the "near" test (ahead of
+        // the point, within the largest edge on each axis) gates the
+        // per-orientation test. Lanes of one item AND their alive sets.
+        const int clo = __reduce_min_sync(FULL, alive ? jsup : INT_MAX);
+        for (int j0 = clo; j0 < nb; j0 += 4 << lg) {
+            int4 bb[4];
+            int bz[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const int j = j0 + (u << lg) + ph;
+                const bool in = j < nb;
+                bb[u] = in ? bx[j] : make_int4(0, 0, 0, 0);
+                bz[u] = in ? bzs[j] : 0;
+            }
+            unsigned near = 0;
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const int j = j0 + (u << lg) + ph;
+                const int4 b = bb[u];
+                const bool nu = alive && j >= jsup && x < b.z && y < b.w && b.x < x + S.wmax &&
+                                b.y < y + S.dmax && bz[u] < z + S.hmax;
+                near |= (nu ? 1u : 0u) << u;
+            }
+            const unsigned todo = __reduce_or_sync(FULL, near);
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                if ((todo >> u) & 1u) {
+                    if ((near >> u) & 1u) {
+                        const int4 b = bb[u];
+#pragma unroll
+                        for (int o = 0; o < 6; o++)
+                            if (b.x < x + S.ow[o] && b.y < y + S.od[o] && bz[u] < z + S.oh[o]) alive &= ~(1u << o);
+                    }
+                }
+            }
+            for (int m = 1; m < span; m <<= 1) alive &= __shfl_xor_sync(FULL, alive, m);
+            if (!__any_sync(FULL, alive != 0)) break;
+        }
+        if (has && ph == 0) {
+            const int p = wi[w + q];
+            st[p] = st_pack(m2, known & ~alive, sok, known);
+            if (z > 0) {
+                sup[p] = a0;
+                sup[C + p] = a1;
+                sup[2 * C + p] = a2;
+                sup[3 * C + p] = a3;
+                sup[4 * C + p] = a4;
+                sup[5 * C + p] = a5;
+            }
+        }
+        w += K;
+        if (GREEDY) {
+            const unsigned bal = __ballot_sync(FULL, has && ph == 0 && alive != 0);
+            if (bal) {
+                first = w - K + ((__ffs(bal) - 1) >> lg);
+                break;
+            }
+        }
+    }
+    __syncwarp();
+    return make_int2(first, w);
+}
+
+// Applies one newly placed box to a valid point's state (C1 OR, C3 contact
+// areas). Returns the new state, or 0 when the support grew onto an
+// orientation whose C1 was never evaluated (the point is re-evaluated).
+__device__ __forceinline__ uint32_t st_apply_box(uint32_t s, int x, int y, int z, int4 B, int Bz, int Bz2,
+                                                 const StepOrs& S, int* sup, int C, int p) {
+    const unsigned m2 = s & 0x3fu, known = (s >> 24) & 0x3fu;
+    unsigned blk = (s >> 8) & 0x3fu, sok = (s >> 16) & 0x3fu;
+    if (Bz2 > z && x < B.z && y < B.w) {
+#pragma unroll
+        for (int o = 0; o < 6; o++)
+            if (B.x < x + S.ow[o] && B.y < y + S.od[o] && Bz < z + S.oh[o]) blk |= 1u << o;
+    }
+    if (z > 0 && Bz2 == z) {
+#pragma unroll
+        for (int o = 0; o < 6; o++) {
+            if ((m2 >> o) & 1u) {
+                const int ox = min(x + S.ow[o], B.z) - max(x, B.x);
+                const int oy = min(y + S.od[o], B.w) - max(y, B.y);
+                if (ox > 0 && oy > 0) {
+                    const int v = sup[o * C + p] + ox * oy;
+                    sup[o * C + p] = v;
+                    if (2LL * v >= (long long)S.wd[o]) sok |= 1u << o;
+                }
+            }
+        }
+        if (sok & m2 & ~known) return 0u;
+    }
+    return st_pack(m2, blk, sok, known);
+}
+
+// Warp: pick the pair, place the box, drop the points it covers and insert
+// its uncovered corners (invalid), then update the top-sorted box tables and
+// the top-z index. pp is the first point holding a feasible pair.
+__device__ __forceinline__ int place1(int t, int pp, bool full, uint32_t* mt, int& mpos, uint32_t* keys,
+                                      uint32_t* st, int* sup, int4* bx, int* bzs, int* z2s,
+                                      unsigned short* bis, unsigned short* zt, int Hz, int& nc, int& nb,
+                                      int P, int C, const StepOrs& S, uint32_t xmask, uint32_t ymask,
+                                      int xb, int xyb, unsigned long long* pass_out, long long& vol,
+                                      int4& Bo, int& Bzo, int& Bz2o, int lane) {
+    int pick = pp;
+    int pick_oi = __ffs(st_feasible(st[pp])) - 1;
+    if (full) {
+        int count = 0;
+        for (int i = pp + lane; i < nc; i += 32) count += __popc(st_feasible(st[i]));
+        count = __reduce_add_sync(FULL, count);
+        const int idx = mt_randrange(mt, mpos, lane, count);
+        if (idx < 0) return ERR_RNG;
+        // idx-th feasible pair in (point, orientation) order
+        int run = 0;
+        for (int cb = pp; cb < nc; cb += 32) {
+            const int i = cb + lane;
+            const unsigned m = i < nc ? st_feasible(st[i]) : 0u;
+            const int c = __popc(m);
+            int inc = c;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const int v = __shfl_up_sync(FULL, inc, d);
+                if (lane >= d) inc += v;
+            }
+            const int tot = __shfl_sync(FULL, inc, 31);
+            if (idx < run + tot) {
+                const unsigned hit = __ballot_sync(FULL, idx < run + inc);
+                const int l = __ffs(hit) - 1;
+                const int excl = __shfl_sync(FULL, inc - c, l);
+                const unsigned ml = __shfl_sync(FULL, m, l);
+                pick = cb + l;
+                pick_oi = __fns(ml, 0, idx - run - excl + 1);
+                break;
+            }
+            run += tot;
+        }
+    }
+    const uint32_t pkey = keys[pick];
+    const int px = (int)(pkey & xmask), py = (int)((pkey >> xb) & ymask), pz = (int)(pkey >> xyb);
+    int pw = 0, pd = 0, ph = 0;
+#pragma unroll
+    for (int o = 0; o < 6; o++)
+        if (o == pick_oi) { pw = S.ow[o]; pd = S.od[o]; ph = S.oh[o]; }
+    const int px2 = px + pw, py2 = py + pd, pz2 = pz + ph;
+    if (nb >= P) return ERR_BOX_CAP;
+    if (lane == 0) pass_out[nb] = pack_place(px, py, pz, pick_oi, t);
+    vol += 1LL * pw * pd * ph;
+    // corners of the new box covered by an already placed box
+    unsigned cov = 1u;   // corner 0 = (px, py, pz): covered by the new box
+    for (int jj = lane; jj < nb; jj += 32) {
+        const int4 b = bx[jj];
+        const int bzb = bzs[jj], bzt = z2s[jj];
+        const unsigned xin = (b.x <= px && px < b.z ? 1u : 0u) | (b.x <= px2 && px2 < b.z ? 2u : 0u);
+        const unsigned yin = (b.y <= py && py < b.w ? 1u : 0u) | (b.y <= py2 && py2 < b.w ? 2u : 0u);
+        const unsigned zin = (bzb <= pz && pz < bzt ? 1u : 0u) | (bzb <= pz2 && pz2 < bzt ? 2u : 0u);
+#pragma unroll
+        for (int c = 0; c < 8; c++)
+            if (((xin >> (c & 1)) & (yin >> ((c >> 1) & 1)) & (zin >> (c >> 2))) & 1u) cov |= 1u << c;
+    }
+    cov = __reduce_or_sync(FULL, cov);
+    // Points covered by the new box have keys >= the pick's (z >= pz, then
+    // y >= py, then x >= px), so only [pick, nc) changes. Survivors move down
+    // in place: every destination is at or below its source, and each round
+    // reads before it writes.
+    int ns = pick;
+    for (int cb = pick; cb < nc; cb += 32) {
+        const int i = cb + lane;
+        bool keep = false;
+        uint32_t key = 0, s = 0;
+        int s0 = 0, s1 = 0, s2 = 0, s3 = 0, s4 = 0, s5 = 0;
+        bool mv_sup = false;
+        if (i < nc) {
+            key = keys[i];
+            const int x = (int)(key & xmask), y = (int)((key >> xb) & ymask), z = (int)(key >> xyb);
+            keep = !(px <= x && x < px2 && py <= y && y < py2 && pz <= z && z < pz2);
+            if (keep) {
+                s = st[i];
+                mv_sup = (s & ST_VALID) && z > 0;
+                if (mv_sup) {
+                    s0 = sup[i]; s1 = sup[C + i]; s2 = sup[2 * C + i];
+                    s3 = sup[3 * C + i]; s4 = sup[4 * C + i]; s5 = sup[5 * C + i];
+                }
+            }
+        }
+        const unsigned bal = __ballot_sync(FULL, keep);
+        __syncwarp();
+        if (keep) {
+            const int d = ns + __popc(bal & lanemask_lt());
+            if (d != i) {
+                keys[d] = key;
+                st[d] = s;
+                if (mv_sup) {
+                    sup[d] = s0; sup[C + d] = s1; sup[2 * C + d] = s2;
+                    sup[3 * C + d] = s3; sup[4 * C + d] = s4; sup[5 * C + d] = s5;
+                }
+            }
+        }
+        ns += __popc(bal);
+    }
+    __syncwarp();
+    // new corners, in index order c = (cz << 2) | (cy << 1) | cx, which is
+    // their (z, y, x) order; all lie after the pick
+    uint32_t ck = 0;
+    int rank = 0;
+    bool isnew = false;
+    if (lane < 8 && !((cov >> lane) & 1u)) {
+        const int cx = (lane & 1) ? px2 : px, cy = (lane & 2) ? py2 : py, cz = (lane & 4) ? pz2 : pz;
+        ck = ((uint32_t)cz << xyb) | ((uint32_t)cy << xb) | (uint32_t)cx;
+        int lo = pick, n = ns - pick;
+        while (n > 0) {
+            const int half = n >> 1;
+            if (keys[lo + half] < ck) { lo += half + 1; n -= half + 1; }
+            else n = half;
+        }
+        rank = lo;
+        isnew = !(lo < ns && keys[lo] == ck);
+    }
+    const unsigned newm = __ballot_sync(FULL, isnew);
+    const int nnew = ns + __popc(newm);
+    if (nnew > C) return ERR_CAND_CAP;
+    if (newm) {
+        const int first_ins = __reduce_min_sync(FULL, isnew ? rank : INT_MAX);
+        uint32_t ckk[8];
+#pragma unroll
+        for (int c = 0; c < 8; c++) ckk[c] = __shfl_sync(FULL, ck, c);
+        // survivors at or after the first insertion move up by the number of
+        // new corners below them; rounds go from the top, reading first
+        for (int hi = ns; hi > first_ins; hi -= 32) {
+            const int i = hi - 1 - lane;
+            const bool in = i >= first_ins;
+            uint32_t key = 0, s = 0;
+            int s0 = 0, s1 = 0, s2 = 0, s3 = 0, s4 = 0, s5 = 0;
+            bool mv_sup = false;
+            int off = 0;
+            if (in) {
+                key = keys[i];
+                s = st[i];
+                mv_sup = (s & ST_VALID) && (key >> xyb) > 0;
+                if (mv_sup) {
+                    s0 = sup[i]; s1 = sup[C + i]; s2 = sup[2 * C + i];
+                    s3 = sup[3 * C + i]; s4 = sup[4 * C + i]; s5 = sup[5 * C + i];
+                }
+#pragma unroll
+                for (int c = 0; c < 8; c++) off += ((newm >> c) & 1u) && ckk[c] < key;
+            }
+            __syncwarp();
+            if (in && off) {
+                const int d = i + off;
+                keys[d] = key;
+                st[d] = s;
+                if (mv_sup) {
+                    sup[d] = s0; sup[C + d] = s1; sup[2 * C + d] = s2;
+                    sup[3 * C + d] = s3; sup[4 * C + d] = s4; sup[5 * C + d] = s5;
+                }
+            }
+            __syncwarp();
+        }
+        if (isnew) {
+            const int d = rank + __popc(newm & ((1u << lane) - 1u));
+            keys[d] = ck;
+            st[d] = 0u;
+        }
+    }
+    nc = nnew;
+    // insert the box into the top-sorted tables (after equal tops)
+    int ip;
+    {
+        int lo = 0, n = nb;
+        while (n > 0) {
+            const int half = n >> 1;
+            if (z2s[lo + half] <= pz2) { lo += half + 1; n -= half + 1; }
+            else n = half;
+        }
+        ip = lo;
+    }
+    for (int hi = nb; hi > ip; hi -= 32) {
+        const int i = hi - 1 - lane;
+        int4 vb = make_int4(0, 0, 0, 0);
+        int vz = 0, vt = 0;
+        unsigned short vi = 0;
+        const bool mv = i >= ip;
+        if (mv) { vb = bx[i]; vz = bzs[i]; vt = z2s[i]; vi = bis[i]; }
+        __syncwarp();
+        if (mv) { bx[i + 1] = vb; bzs[i + 1] = vz; z2s[i + 1] = vt; bis[i + 1] = vi; }
+        __syncwarp();
+    }
+    if (lane == 0) {
+        bx[ip] = make_int4(px, py, px2, py2);
+        bzs[ip] = pz;
+        z2s[ip] = pz2;
+        bis[ip] = (unsigned short)nb;
+    }
+    if (zt)
+        for (int zz = pz2 + 1 + lane; zz < Hz; zz += 32) zt[zz]++;
+    nb++;
+    Bo = make_int4(px, py, px2, py2);
+    Bzo = pz;
+    Bz2o = pz2;
+    __syncwarp();
+    return ERR_NONE;
+}
+
+__device__ __forceinline__ void decoder1_body(const DecoderArgs& a, unsigned char* base, int gdec) {
+    const int lane = threadIdx.x & 31;
+    const Dec1Layout lay = dec1_layout(a.P, a.C, a.Hz);
+    const int C = a.C;
+    uint32_t* mt = reinterpret_cast<uint32_t*>(base);
+    int4* bx = reinterpret_cast<int4*>(base + lay.off_bx);
+    int* bzs = reinterpret_cast<int*>(base + lay.off_bz);
+    int* z2s = reinterpret_cast<int*>(base + lay.off_z2);
+    unsigned short* bis = reinterpret_cast<unsigned short*>(base + lay.off_bi);
+    uint32_t* keys = reinterpret_cast<uint32_t*>(base + lay.off_key);
+    uint32_t* st = reinterpret_cast<uint32_t*>(base + lay.off_st);
+    int* sup = reinterpret_cast<int*>(base + lay.off_sup);
+    uint2* Wl = reinterpret_cast<uint2*>(base + lay.off_w);
+    unsigned short* wi = reinterpret_cast<unsigned short*>(base + lay.off_wi);
+    unsigned short* zt = a.Hz ? reinterpret_cast<unsigned short*>(base + lay.off_zt) : nullptr;
+
+    for (;;) {
+        if (*reinterpret_cast<volatile int*>(a.abort)) return;
+        int item = 0;
+        if (lane == 0) item = atomicAdd(a.work_next, 1);
+        item = __shfl_sync(FULL, item, 0);
+        if (item >= a.n_work) break;
+        const int2 wk = a.work[item];
+        const InstDesc I = a.inst[wk.x];
+        const int restart = wk.y;
+        const int slot = I.slot_base + restart;
+        const int L = I.L, W = I.W, H = I.H;
+        const uint32_t xmask = (1u << I.xb) - 1u, ymask = (1u << I.yb) - 1u;
+        const int xb = I.xb, xyb = I.xb + I.yb;
+        const bool randomized = !(I.first_fit || I.eps == 0.0);
+        unsigned long long* best_out = a.places + I.place_off + (long long)restart * I.place_stride;
+        unsigned long long* pass_out =
+            I.passes > 1 ? a.scratch + (long long)gdec * I.place_stride : best_out;
+        int mpos = 624;
+        {
+            const long long sd = I.seed + restart;
+            mt_seed_warp(mt, (unsigned long long)(sd < 0 ? -sd : sd), a.mt_init, lane);
+        }
+        int err = ERR_NONE;
+        bool have_acc = false, have_any = false;
+        long long best_vol = 0;
+        int best_n = 0;
+        double best_score = 0.0;
+
+        for (int pass = 0; pass < I.passes && err == ERR_NONE; pass++) {
+            int nb = 0, nc = 1;
+            long long vol = 0;
+            if (zt)
+                for (int i = lane; i < a.Hz; i += 32) zt[i] = 0;
+            if (lane == 0) {
+                keys[0] = 0u;
+                st[0] = 0u;
+            }
+            __syncwarp();
+            int state_type = -1;
+            bool pending = false;   // a placed box not yet applied to the valid states
+            int4 B = make_int4(0, 0, 0, 0);
+            int Bz = 0, Bz2 = 0;
+            for (int sti = 0; sti < I.n_steps; sti++) {
+                const int t = a.step_type[I.step_off + sti];
+                const TypeOrs& T = a.types[I.type_off + t];
+                StepOrs S;
+                S.no = T.n;
+                if (S.no == 0) continue;
+                S.wmax = S.dmax = S.hmax = 0;
+#pragma unroll
+                for (int o = 0; o < 6; o++) {
+                    S.ow[o] = T.w[o];
+                    S.od[o] = T.d[o];
+                    S.oh[o] = T.h[o];
+                    S.wd[o] = S.ow[o] * S.od[o];
+                    S.wmax = max(S.wmax, S.ow[o]);
+                    S.dmax = max(S.dmax, S.od[o]);
+                    S.hmax = max(S.hmax, S.oh[o]);
+                }
+                const bool fresh = t != state_type;
+                state_type = t;
+                const bool apply = pending && !fresh;
+                pending = false;
+                // filter: bring valid states up to date with the last box and
+                // read their feasible sets; list the invalid points that have an
+                // orientation inside the container and, above the floor, a box
+                // top at their height. v = first valid point with a feasible pair.
+                int nW = 0, v = INT_MAX, nWg = -1;
+                for (int cb = 0; cb < nc; cb += 32) {
+                    const int i = cb + lane;
+                    unsigned f = 0;
+                    bool cand = false;
+                    uint2 it = make_uint2(0, 0);
+                    if (i < nc) {
+                        const uint32_t key = keys[i];
+                        const int x = (int)(key & xmask), y = (int)((key >> xb) & ymask), z = (int)(key >> xyb);
+                        uint32_t s = fresh ? 0u : st[i];
+                        const uint32_t s_in = s;
+                        if ((s & ST_VALID) && apply) s = st_apply_box(s, x, y, z, B, Bz, Bz2, S, sup, C, i);
+                        if (s & ST_VALID) {
+                            f = st_feasible(s);
+                        } else {
+                            unsigned m = 0;
+#pragma unroll
+                            for (int o = 0; o < 6; o++)
+                                if (o < S.no && x + S.ow[o] <= L && y + S.od[o] <= W && z + S.oh[o] <= H) m |= 1u << o;
+                            if (!m) {
+                                s = ST_VALID;   // nothing fits: infeasible for the rest of the run
+                            } else {
+                                s = 0u;
+                                const int jlo = box_start(zt, z2s, nb, z);
+                                const int jsup = z > 0 ? box_start(zt, z2s, nb, z + 1) : jlo;
+                                if (z == 0 || jsup > jlo) {
+                                    cand = true;
+                                    it = make_item(key, m, jlo, jsup);
+                                }
+                            }
+                        }
+                        if (s != s_in || fresh) st[i] = s;
+                    }
+                    const unsigned bal = __ballot_sync(FULL, cand);
+                    if (v == INT_MAX) {
+                        const unsigned bf = __ballot_sync(FULL, f != 0);
+                        if (bf) {
+                            v = cb + __ffs(bf) - 1;
+                            nWg = nW + __popc(bal & ((1u << (v - cb)) - 1u));
+                        }
+                    }
+                    if (cand) {
+                        const int d = nW + __popc(bal & lanemask_lt());
+                        Wl[d] = it;
+                        wi[d] = (unsigned short)i;
+                    }
+                    nW += __popc(bal);
+                }
+                if (nWg < 0) nWg = nW;
+                __syncwarp();
+                // greedy: the invalid points before v, in order
+                int pp = v, wend = 0;
+                if (nWg > 0) {
+                    const int2 r = eval_items<true>(Wl, wi, 0, nWg, bx, bzs, nb, S, xmask, ymask, xb, xyb,
+                                                    st, sup, C, lane);
+                    if (r.x != INT_MAX) pp = wi[r.x];
+                    wend = r.y;
+                }
+                if (pp == INT_MAX) continue;             // no feasible pair: no draw
+                const bool full = randomized && mt_random(mt, mpos, lane) >= 1.0 - I.eps;
+                if (full && wend < nW)                   // every feasible pair is needed
+                    eval_items<false>(Wl, wi, wend, nW, bx, bzs, nb, S, xmask, ymask, xb, xyb, st, sup, C,
+                                      lane);
+                err = place1(t, pp, full, mt, mpos, keys, st, sup, bx, bzs, z2s, bis, zt, a.Hz, nc, nb, a.P,
+                             C, S, xmask, ymask, xb, xyb, pass_out, vol, B, Bz, Bz2, lane);
+                if (err != ERR_NONE) break;
+                pending = true;
+            }
+            if (err != ERR_NONE) break;
+            const double score =
+                fsr_score_warp(bx, bzs, z2s, bis, nb, I.mu, reinterpret_cast<char*>(keys), lane, nullptr);
+            const bool acc = !I.has_theta || score >= I.theta;
+            bool take;
+            if (acc) take = !have_acc || vol > best_vol || (vol == best_vol && nb > best_n);
+            else take = !have_acc && (!have_any || vol > best_vol || (vol == best_vol && nb > best_n));
+            if (take) {
+                best_vol = vol;
+                best_n = nb;
+                best_score = score;
+                if (pass_out != best_out)
+                    for (int i = lane; i < nb; i += 32) best_out[i] = pass_out[i];
+            }
+            have_any = true;
+            have_acc = have_acc || acc;
+            __syncwarp();
+        }
+        if (lane == 0) {
+            if (err) atomicOr(a.err_flag, 1 << err);
+            SlotHead h;
+            h.n_boxes = err ? 0 : best_n;
+            h.err = err;
+            h.volume = err ? 0 : best_vol;
+            h.score = err ? 0.0 : best_score;
+            h.n_passes = I.passes;
+            h.fallback = have_acc ? 0 : 1;
+            a.heads[slot] = h;
+        }
+        __syncwarp();
+    }
+}
+
+template <int D, int M>
+__global__ void __launch_bounds__(32 * D, M) decoder1_kernel(DecoderArgs a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int dec = threadIdx.x >> 5;
+    const Dec1Layout lay = dec1_layout(a.P, a.C, a.Hz);
+    decoder1_body(a, smem_raw + (size_t)dec * lay.bytes, blockIdx.x * D + dec);
+}
+
+// ---------------------------------------------------------------------------
 // per-instance best restart: accepted first, then max (volume, n_boxes),
 // earliest restart on ties (the strict > of gpu/plp_common.hpp:507-511)
 // ---------------------------------------------------------------------------
@@ -992,15 +1623,22 @@ __global__ void gather_best_kernel(const InstDesc* __restrict__ inst, int n_inst
 // (G warps per decoder, D decoders per CTA, M minimum resident CTAs per SM:
 // a register cap of 65536 / (32 G D M) per thread) instantiations
 #define PLP_DECODER_CONFIGS(X)                                                                 \
-    X(1, 2, 1) X(1, 4, 1) X(1, 4, 4) X(1, 8, 1) X(1, 8, 2) X(2, 1, 1) X(2, 2, 1) X(2, 2, 5)     \
+    X(1, 1, 1) X(1, 2, 1) X(1, 4, 1) X(1, 4, 4) X(1, 8, 1) X(1, 8, 2) X(2, 1, 1) X(2, 2, 1) X(2, 2, 5)     \
     X(2, 4, 1) X(2, 4, 3) X(4, 1, 1) X(4, 1, 5) X(4, 1, 6) X(4, 2, 1) X(4, 2, 3) X(4, 4, 1)   \
     X(8, 1, 1) X(8, 1, 3) X(8, 2, 1)
 
 using DecoderFn = void (*)(DecoderArgs);
 
+// G = 1: the incremental single-warp decoder; G > 1: the multi-warp decoder
+template <int G, int D, int M>
+static DecoderFn pick_kernel() {
+    if constexpr (G == 1) return decoder1_kernel<D, M>;
+    else return decoder_kernel<G, D, M>;
+}
+
 static DecoderFn decoder_fn(int G, int D, int M) {
 #define PLP_PICK(g, d, m) \
-    if (G == g && D == d && M == m) return decoder_kernel<g, d, m>;
+    if (G == g && D == d && M == m) return pick_kernel<g, d, m>();
     PLP_DECODER_CONFIGS(PLP_PICK)
 #undef PLP_PICK
     return nullptr;
@@ -1027,7 +1665,7 @@ cudaError_t launch_decoder(const DecodeLaunch& L, cudaStream_t st) {
     a.P = L.P;
     a.C = L.C;
     a.Hz = L.Hz;
-    const int smem = decoder_smem_bytes(L.P, L.C, L.Hz) * L.decoders_per_cta;
+    const int smem = decoder_smem_bytes(L.P, L.C, L.Hz, L.warps_per_decoder) * L.decoders_per_cta;
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
     e = cudaMemsetAsync(L.work_next, 0, sizeof(int), st);
@@ -1041,7 +1679,7 @@ cudaError_t launch_decoder(const DecodeLaunch& L, cudaStream_t st) {
 cudaError_t decoder_occupancy(int P, int C, int Hz, int G, int D, int M, int* ctas_per_sm) {
     DecoderFn fn = decoder_fn(G, D, M);
     if (!fn) return cudaErrorInvalidConfiguration;
-    const int smem = decoder_smem_bytes(P, C, Hz) * D;
+    const int smem = decoder_smem_bytes(P, C, Hz, G) * D;
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas_per_sm, fn, 32 * G * D, smem);

@@ -28,7 +28,7 @@ struct DecodeLaunch {
     int ctas;
 };
 
-int decoder_smem_bytes(int P, int C, int Hz);
+int decoder_smem_bytes(int P, int C, int Hz, int G);
 bool decoder_config_supported(int G, int D, int M);
 cudaError_t decoder_occupancy(int P, int C, int Hz, int G, int D, int M, int* ctas_per_sm);
 cudaError_t launch_decoder(const DecodeLaunch& L, cudaStream_t st);
