@@ -159,7 +159,7 @@ struct DecoderArgs {
 // the supports j are updated in parallel (each j by one lane), so every
 // load[j] receives its additions in the reference order.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ double fsr_score_warp(const int4* bx, const int* bz, const int* z2,
+static __device__ __noinline__ double fsr_score_warp(const int4* bx, const int* bz, const int* z2,
                                  const unsigned short* bi, int n, double mu, char* scratch,
                                  int lane, double* fsr_out) {
     if (n == 0) return 0.0;
@@ -888,8 +888,7 @@ __device__ __forceinline__ unsigned st_feasible(uint32_t s) {
 // items at a time, lg chosen so that a short item list still spreads over the
 // whole warp. Greedy mode stops after the first group holding a feasible
 // item. Returns {first feasible item or INT_MAX, end of the evaluated range}.
-template <bool GREEDY>
-__device__ __forceinline__ int2 eval_items(const uint2* W, const unsigned short* wi, int w0, int w1,
+__device__ __forceinline__ int2 eval_items(const bool GREEDY, const uint2* W, const unsigned short* wi, int w0, int w1,
                                            const int4* bx, const int* bzs, int nb, const StepOrs& S,
                                            uint32_t xmask, uint32_t ymask, int xb, int xyb,
                                            uint32_t* st, int* sup, int C, int lane) {
@@ -1096,19 +1095,54 @@ __device__ __forceinline__ int place1(int t, int pp, bool full, uint32_t* mt, in
     if (nb >= P) return ERR_BOX_CAP;
     if (lane == 0) pass_out[nb] = pack_place(px, py, pz, pick_oi, t);
     vol += 1LL * pw * pd * ph;
-    // corners of the new box covered by an already placed box
+    // Box tables, one pass from the top: the corners of the new box that a
+    // placed box covers, and the boxes whose top is above the new box's move
+    // up one slot (each round reads before it writes, and writes only slots
+    // it or an earlier round has read).
     unsigned cov = 1u;   // corner 0 = (px, py, pz): covered by the new box
-    for (int jj = lane; jj < nb; jj += 32) {
-        const int4 b = bx[jj];
-        const int bzb = bzs[jj], bzt = z2s[jj];
-        const unsigned xin = (b.x <= px && px < b.z ? 1u : 0u) | (b.x <= px2 && px2 < b.z ? 2u : 0u);
-        const unsigned yin = (b.y <= py && py < b.w ? 1u : 0u) | (b.y <= py2 && py2 < b.w ? 2u : 0u);
-        const unsigned zin = (bzb <= pz && pz < bzt ? 1u : 0u) | (bzb <= pz2 && pz2 < bzt ? 2u : 0u);
+    int nabove = 0;
+    for (int hi = nb; hi > 0; hi -= 32) {
+        const int jj = hi - 1 - lane;
+        const bool in = jj >= 0;
+        int4 b = make_int4(0, 0, 0, 0);
+        int bzb = 0, bzt = 0;
+        unsigned short bi = 0;
+        if (in) {
+            b = bx[jj];
+            bzb = bzs[jj];
+            bzt = z2s[jj];
+            bi = bis[jj];
+            const unsigned xin = (b.x <= px && px < b.z ? 1u : 0u) | (b.x <= px2 && px2 < b.z ? 2u : 0u);
+            const unsigned yin = (b.y <= py && py < b.w ? 1u : 0u) | (b.y <= py2 && py2 < b.w ? 2u : 0u);
+            const unsigned zin = (bzb <= pz && pz < bzt ? 1u : 0u) | (bzb <= pz2 && pz2 < bzt ? 2u : 0u);
 #pragma unroll
-        for (int c = 0; c < 8; c++)
-            if (((xin >> (c & 1)) & (yin >> ((c >> 1) & 1)) & (zin >> (c >> 2))) & 1u) cov |= 1u << c;
+            for (int c = 0; c < 8; c++)
+                if (((xin >> (c & 1)) & (yin >> ((c >> 1) & 1)) & (zin >> (c >> 2))) & 1u) cov |= 1u << c;
+        }
+        const bool up = in && bzt > pz2;
+        nabove += __popc(__ballot_sync(FULL, up));
+        __syncwarp();
+        if (up) {
+            bx[jj + 1] = b;
+            bzs[jj + 1] = bzb;
+            z2s[jj + 1] = bzt;
+            bis[jj + 1] = bi;
+        }
     }
     cov = __reduce_or_sync(FULL, cov);
+    {
+        const int ip = nb - nabove;   // after the boxes with equal tops
+        __syncwarp();
+        if (lane == 0) {
+            bx[ip] = make_int4(px, py, px2, py2);
+            bzs[ip] = pz;
+            z2s[ip] = pz2;
+            bis[ip] = (unsigned short)nb;
+        }
+    }
+    if (zt)
+        for (int zz = pz2 + 1 + lane; zz < Hz; zz += 32) zt[zz]++;
+    nb++;
     // Points covered by the new box have keys >= the pick's (z >= pz, then
     // y >= py, then x >= px), so only [pick, nc) changes. Survivors move down
     // in place: every destination is at or below its source, and each round
@@ -1213,37 +1247,6 @@ __device__ __forceinline__ int place1(int t, int pp, bool full, uint32_t* mt, in
         }
     }
     nc = nnew;
-    // insert the box into the top-sorted tables (after equal tops)
-    int ip;
-    {
-        int lo = 0, n = nb;
-        while (n > 0) {
-            const int half = n >> 1;
-            if (z2s[lo + half] <= pz2) { lo += half + 1; n -= half + 1; }
-            else n = half;
-        }
-        ip = lo;
-    }
-    for (int hi = nb; hi > ip; hi -= 32) {
-        const int i = hi - 1 - lane;
-        int4 vb = make_int4(0, 0, 0, 0);
-        int vz = 0, vt = 0;
-        unsigned short vi = 0;
-        const bool mv = i >= ip;
-        if (mv) { vb = bx[i]; vz = bzs[i]; vt = z2s[i]; vi = bis[i]; }
-        __syncwarp();
-        if (mv) { bx[i + 1] = vb; bzs[i + 1] = vz; z2s[i + 1] = vt; bis[i + 1] = vi; }
-        __syncwarp();
-    }
-    if (lane == 0) {
-        bx[ip] = make_int4(px, py, px2, py2);
-        bzs[ip] = pz;
-        z2s[ip] = pz2;
-        bis[ip] = (unsigned short)nb;
-    }
-    if (zt)
-        for (int zz = pz2 + 1 + lane; zz < Hz; zz += 32) zt[zz]++;
-    nb++;
     Bo = make_int4(px, py, px2, py2);
     Bzo = pz;
     Bz2o = pz2;
@@ -1384,19 +1387,26 @@ __device__ __forceinline__ void decoder1_body(const DecoderArgs& a, unsigned cha
                 }
                 if (nWg < 0) nWg = nW;
                 __syncwarp();
-                // greedy: the invalid points before v, in order
-                int pp = v, wend = 0;
-                if (nWg > 0) {
-                    const int2 r = eval_items<true>(Wl, wi, 0, nWg, bx, bzs, nb, S, xmask, ymask, xb, xyb,
-                                                    st, sup, C, lane);
-                    if (r.x != INT_MAX) pp = wi[r.x];
-                    wend = r.y;
+                // greedy: the invalid points before v, in order; then, on the
+                // random branch, every item left (one evaluation site)
+                int pp = v, lo = 0, hi = nWg;
+                bool greedy = true, full = false;
+                for (;;) {
+                    if (lo < hi) {
+                        const int2 r = eval_items(greedy, Wl, wi, lo, hi, bx, bzs, nb, S, xmask, ymask, xb, xyb,
+                                                  st, sup, C, lane);
+                        if (greedy) {
+                            if (r.x != INT_MAX) pp = wi[r.x];
+                            lo = r.y;
+                        }
+                    }
+                    if (!greedy || pp == INT_MAX) break;
+                    full = randomized && mt_random(mt, mpos, lane) >= 1.0 - I.eps;
+                    if (!full || lo >= nW) break;
+                    greedy = false;   // every feasible pair is needed
+                    hi = nW;
                 }
                 if (pp == INT_MAX) continue;             // no feasible pair: no draw
-                const bool full = randomized && mt_random(mt, mpos, lane) >= 1.0 - I.eps;
-                if (full && wend < nW)                   // every feasible pair is needed
-                    eval_items<false>(Wl, wi, wend, nW, bx, bzs, nb, S, xmask, ymask, xb, xyb, st, sup, C,
-                                      lane);
                 err = place1(t, pp, full, mt, mpos, keys, st, sup, bx, bzs, z2s, bis, zt, a.Hz, nc, nb, a.P,
                              C, S, xmask, ymask, xb, xyb, pass_out, vol, B, Bz, Bz2, lane);
                 if (err != ERR_NONE) break;

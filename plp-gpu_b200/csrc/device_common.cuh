@@ -92,7 +92,7 @@ __device__ __forceinline__ unsigned lanemask_lt() {
 // init_by_array on |seed| (one or two 32-bit key words), starting from the
 // seed-independent init_genrand(19650218) table `init`. The recurrence is
 // serial: lane 0 runs it, the warp then syncs.
-__device__ inline void mt_seed_warp(uint32_t* mt, unsigned long long seed_abs,
+static __device__ __noinline__ void mt_seed_warp(uint32_t* mt, unsigned long long seed_abs,
                                     const uint32_t* __restrict__ init, int lane) {
     for (int i = lane; i < 624; i += 32) mt[i] = init[i];
     __syncwarp();
@@ -126,7 +126,7 @@ __device__ inline void mt_seed_warp(uint32_t* mt, unsigned long long seed_abs,
 // (i + 397) mod 624, which is still old for i < 227 and already new for
 // i >= 227. Chunks of 32 in increasing i therefore only read finished or
 // untouched words; inside a chunk all lanes read before any lane writes.
-__device__ inline void mt_twist_warp(uint32_t* mt, int lane) {
+static __device__ __noinline__ void mt_twist_warp(uint32_t* mt, int lane) {
     for (int base = 0; base < 623; base += 32) {
         const int i = base + lane;
         uint32_t nv = 0;
