@@ -1312,8 +1312,10 @@ __device__ __forceinline__ void decoder1_body(const DecoderArgs& a, unsigned cha
             bool pending = false;   // a placed box not yet applied to the valid states
             int4 B = make_int4(0, 0, 0, 0);
             int Bz = 0, Bz2 = 0;
+            int t_next = I.n_steps > 0 ? a.step_type[I.step_off] : 0;
             for (int sti = 0; sti < I.n_steps; sti++) {
-                const int t = a.step_type[I.step_off + sti];
+                const int t = t_next;
+                if (sti + 1 < I.n_steps) t_next = a.step_type[I.step_off + sti + 1];
                 const TypeOrs& T = a.types[I.type_off + t];
                 StepOrs S;
                 S.no = T.n;

@@ -97,25 +97,49 @@ static __device__ __noinline__ void mt_seed_warp(uint32_t* mt, unsigned long lon
     for (int i = lane; i < 624; i += 32) mt[i] = init[i];
     __syncwarp();
     if (lane == 0) {
+        // Key word j of step k is k mod nkey; its addend is key[j] + j.
         const uint32_t k0 = (uint32_t)seed_abs;
         const uint32_t k1 = (uint32_t)(seed_abs >> 32);
-        const int nkey = k1 ? 2 : 1;
+        const uint32_t add0 = k0, add1 = k1 ? k1 + 1u : k0;
+        // First loop: 624 steps over i = 1 .. 623, then i = 1 again. Blocks
+        // of 8 with their old words loaded up front keep the load latency
+        // off the serial chain.
         uint32_t prev = mt[0];
-        int i = 1, j = 0;
-        for (int k = 624; k > 0; k--) {
-            const uint32_t t = prev ^ (prev >> 30);
-            const uint32_t v = (mt[i] ^ (t * 1664525u)) + (j ? k1 : k0) + (uint32_t)j;
-            mt[i] = v;
-            prev = v;
-            if (++i >= 624) { mt[0] = v; i = 1; }
-            if (++j >= nkey) j = 0;
+        for (int i = 1; i < 624; i += 8) {
+            uint32_t o[8];
+#pragma unroll
+            for (int u = 0; u < 8; u++) o[u] = i + u < 624 ? mt[i + u] : 0u;
+#pragma unroll
+            for (int u = 0; u < 8; u++) {
+                if (i + u < 624) {
+                    const uint32_t t = prev ^ (prev >> 30);
+                    prev = (o[u] ^ (t * 1664525u)) + (((i + u - 1) & 1) ? add1 : add0);
+                    mt[i + u] = prev;
+                }
+            }
         }
-        for (int k = 623; k > 0; k--) {
+        {
             const uint32_t t = prev ^ (prev >> 30);
-            const uint32_t v = (mt[i] ^ (t * 1566083941u)) - (uint32_t)i;
-            mt[i] = v;
-            prev = v;
-            if (++i >= 624) { mt[0] = v; i = 1; }
+            prev = (mt[1] ^ (t * 1664525u)) + add1;   // step 623 (odd)
+            mt[1] = prev;
+        }
+        // Second loop: 623 steps over i = 2 .. 623, then i = 1.
+        for (int i = 2; i < 624; i += 8) {
+            uint32_t o[8];
+#pragma unroll
+            for (int u = 0; u < 8; u++) o[u] = i + u < 624 ? mt[i + u] : 0u;
+#pragma unroll
+            for (int u = 0; u < 8; u++) {
+                if (i + u < 624) {
+                    const uint32_t t = prev ^ (prev >> 30);
+                    prev = (o[u] ^ (t * 1566083941u)) - (uint32_t)(i + u);
+                    mt[i + u] = prev;
+                }
+            }
+        }
+        {
+            const uint32_t t = prev ^ (prev >> 30);
+            mt[1] = (mt[1] ^ (t * 1566083941u)) - 1u;
         }
         mt[0] = 0x80000000u;
     }
