@@ -164,11 +164,20 @@ void plp_destroy(plp_handle* h);
  * live-point depth C (per decoder, in shared memory; C a multiple of 32),
  * warps per decoder G, decoders per CTA D and minimum resident CTAs per SM M
  * (which caps registers per thread at 65536 / (32 G D M)). (G, D, M) must be
- * one of (1,2,1) (1,4,1) (1,4,4) (1,8,1) (1,8,2) (2,1,1) (2,2,1) (2,2,5)
+ * one of (1,1,1) (1,2,1) (1,4,1) (1,4,4) (1,8,1) (1,8,2) (2,1,1) (2,2,1) (2,2,5)
  * (2,4,1) (2,4,3) (4,1,1) (4,1,5) (4,1,6) (4,2,1) (4,2,3) (4,4,1) (8,1,1)
  * (8,1,3) (8,2,1); 0 keeps the current value. Restarts that outgrow the tile
  * are re-run with a deeper one, so the tile affects speed only, never results. */
 int plp_set_tile(plp_handle* h, int32_t P, int32_t C, int32_t G, int32_t D, int32_t M);
+
+/* Autotuner (no reference counterpart): times candidate tiles -- one warp per
+ * decoder with placed-box depth P, live-point depth C, decoders per CTA D and
+ * minimum CTAs per SM M -- on a strided sample of at most max_decodes of the
+ * workload's decodes (0 = 8192), each after a warm-up run, and keeps the
+ * fastest as the handle's tile. tile_out (may be NULL) receives {P, C, G, D, M}.
+ * The tile never changes results. */
+int plp_autotune(plp_handle* h, const plp_instance* const* insts, int32_t n_inst,
+                 const plp_run_opts* opts, int32_t n_opts, int32_t max_decodes, int32_t* tile_out);
 
 /* Synchronous batched solve: every restart of every instance in one
  * persistent decoder launch (plus a FSR/selection launch), results copied to
@@ -180,7 +189,10 @@ int plp_solve(plp_handle* h, const plp_instance* const* insts, int32_t n_inst,
  * caller can run the device part repeatedly (timing) and fetch results when
  * it wants them. plp_batch_run is synchronous; device_ms is the CUDA-event
  * time of all device work of the run, decoder_ms that of the decoder kernel
- * alone, launches the number of kernels launched. */
+ * alone, launches the number of kernels launched. A run that needed no
+ * capacity retry is captured as one CUDA graph (error-flag reset, decoder,
+ * flag copy, selection, gather) and later runs with the same tile replay it
+ * with a single graph launch and a single synchronisation. */
 typedef struct plp_batch plp_batch;
 int plp_batch_prepare(plp_handle* h, const plp_instance* const* insts, int32_t n_inst,
                       const plp_run_opts* opts, int32_t n_opts, plp_batch** out);
@@ -189,6 +201,9 @@ int plp_batch_run(plp_batch* b, double* device_ms, double* decoder_ms, int32_t* 
 int plp_batch_fetch(plp_batch* b, plp_result** results);
 /* bytes the batch copies host->device (tables) and device->host (results) */
 int plp_batch_io_bytes(const plp_batch* b, int64_t* h2d, int64_t* d2h);
+/* 1 when the batch's next run replays its captured CUDA graph, else 0 (no
+ * reference counterpart). */
+int plp_batch_graph(const plp_batch* b);
 void plp_batch_free(plp_batch* b);
 
 /* Serving: admit a request; it starts as soon as the memory budget allows and

@@ -139,6 +139,11 @@ struct Batch {
     size_t scratch_bytes = 0;
     int ctas = 0;
     TileConfig tile;
+    // one-graph replay of a clean execution (flag reset, decoder, flag copy,
+    // select, gather), kept for later executions with the same tile
+    cudaGraphExec_t gexec = nullptr;
+    TileConfig gtile;
+    int glaunches = 0;
     // host results
     std::vector<SlotHead> heads;
     std::vector<int2> best;
@@ -291,6 +296,10 @@ struct ExecStats {
 };
 
 int batch_release(Batch& b, cudaStream_t st) {
+    if (b.gexec) {
+        cudaGraphExecDestroy(b.gexec);
+        b.gexec = nullptr;
+    }
     cudaError_t e = cudaSuccess;
     if (b.d_mem) e = cudaFreeAsync(b.d_mem, st);
     b.d_mem = nullptr;
@@ -370,8 +379,75 @@ static DecodeLaunch make_launch(const Batch& b, const TileConfig& t, const int2*
     return L;
 }
 
-// tile: in = tile to use, out = tile that succeeded (deeper after retries)
-int batch_execute(Batch& b, cudaStream_t st, int sms, TileConfig& tile, ExecStats* xs) {
+bool same_tile(const TileConfig& a, const TileConfig& b) {
+    return a.P == b.P && a.C == b.C && a.G == b.G && a.D == b.D && a.M == b.M;
+}
+
+// After-decoder part of an execution: best restart per instance and, for
+// best-only batches, the gather of its placements.
+cudaError_t enqueue_select(Batch& b, cudaStream_t st, int* launches) {
+    int2* d_best = reinterpret_cast<int2*>(b.d_mem + b.o_best);
+    const InstDesc* d_inst = reinterpret_cast<const InstDesc*>(b.d_mem + b.o_desc);
+    const SlotHead* d_heads = reinterpret_cast<const SlotHead*>(b.d_mem + b.o_heads);
+    cudaError_t e = launch_select_best(d_inst, (int)b.desc.size(), d_heads, d_best, st);
+    if (e != cudaSuccess) return e;
+    (*launches)++;
+    if (b.best_only) {
+        unsigned long long* d_g = reinterpret_cast<unsigned long long*>(b.d_mem + b.o_gather);
+        e = launch_gather_best(d_inst, (int)b.desc.size(), d_best,
+                               reinterpret_cast<const unsigned long long*>(b.d_mem + b.o_places), d_g,
+                               b.max_stride, st);
+        if (e != cudaSuccess) return e;
+        (*launches)++;
+    }
+    return cudaSuccess;
+}
+
+// Records a clean execution of the batch with tile t as one CUDA graph:
+// error-flag reset, the persistent decoder, the flag copy to the pinned word,
+// selection and gather, with event ev[1] between decoder and selection. A
+// capture that fails leaves the batch on direct launches.
+void batch_capture(Batch& b, cudaStream_t st, int sms, const TileConfig& t) {
+    if (b.gexec) {
+        cudaGraphExecDestroy(b.gexec);
+        b.gexec = nullptr;
+    }
+    const DecodeLaunch L = make_launch(b, t, reinterpret_cast<const int2*>(b.d_mem + b.o_work),
+                                       (int)b.work.size(), sms);   // occupancy query: before capture
+    if (configure_decoder(L) != cudaSuccess) {
+        cudaGetLastError();
+        return;
+    }
+    int* d_flag = reinterpret_cast<int*>(b.d_mem + b.o_next + 8);
+    if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        cudaGetLastError();
+        return;
+    }
+    int n = 0;
+    cudaError_t e = cudaMemsetAsync(d_flag, 0, 8, st);
+    if (e == cudaSuccess) e = enqueue_decoder(L, st);
+    if (e == cudaSuccess) n++;
+    if (e == cudaSuccess) e = cudaEventRecord(b.ev[1], st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(b.h_flag, d_flag, 4, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = enqueue_select(b, st, &n);
+    cudaGraph_t g = nullptr;
+    const cudaError_t e2 = cudaStreamEndCapture(st, &g);
+    if (e == cudaSuccess && e2 == cudaSuccess && g) {
+        cudaGraphExec_t x = nullptr;
+        if (cudaGraphInstantiate(&x, g, 0) == cudaSuccess) {
+            b.gexec = x;
+            b.gtile = t;
+            b.glaunches = n;
+        }
+    }
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();
+}
+
+// tile: in = tile to use, out = tile that succeeded (deeper after retries).
+// graph: capture a clean execution and replay it on later calls (batches
+// that run more than once).
+int batch_execute(Batch& b, cudaStream_t st, int sms, TileConfig& tile, ExecStats* xs, bool graph) {
     auto fail = [&](const char* what, cudaError_t err) {
         const int s = set_cuda_error(what, err);
         std::string keep = plpb_last();
@@ -382,6 +458,29 @@ int batch_execute(Batch& b, cudaStream_t st, int sms, TileConfig& tile, ExecStat
     ExecStats x;
     TileConfig t = tile;
     fit_tile(t, b.Hz);
+    if (b.gexec && same_tile(t, b.gtile)) {
+        // replay: one graph launch, one synchronisation
+        cudaError_t e = cudaEventRecord(b.ev[0], st);
+        if (e == cudaSuccess) e = cudaGraphLaunch(b.gexec, st);
+        if (e == cudaSuccess) e = cudaEventRecord(b.ev[2], st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return fail("graph execution", e);
+        if (*reinterpret_cast<volatile int*>(b.h_flag) == 0) {
+            float ms = 0, dms = 0;
+            cudaEventElapsedTime(&ms, b.ev[0], b.ev[2]);
+            if (cudaEventElapsedTime(&dms, b.ev[0], b.ev[1]) != cudaSuccess) {
+                cudaGetLastError();
+                dms = ms;
+            }
+            x.device_ms = ms;
+            x.decoder_ms = dms;
+            x.launches = b.glaunches;
+            tile = t;
+            if (xs) *xs = x;
+            return PLP_OK;
+        }
+        // an error flag: run again on direct launches, which handle it
+    }
     const int2* d_work = reinterpret_cast<const int2*>(b.d_mem + b.o_work);
     int* d_flag = reinterpret_cast<int*>(b.d_mem + b.o_next + 8);
     cudaError_t e = cudaMemsetAsync(d_flag, 0, 8, st);
@@ -399,7 +498,9 @@ int batch_execute(Batch& b, cudaStream_t st, int sms, TileConfig& tile, ExecStat
     x.decoder_ms = ms;
     // capacity retries: restarts whose live points or boxes outgrew the tile
     // run again with a deeper tile (same slots, so results land in place)
+    bool retried = false;
     for (int attempt = 0; *reinterpret_cast<volatile int*>(b.h_flag) != 0; attempt++) {
+        retried = true;
         if (*reinterpret_cast<volatile int*>(b.h_flag) & (1 << ERR_RNG)) {
             batch_release(b, st);
             return set_error(PLP_E_DEVICE, "decoder reported an RNG rejection-bound error");
@@ -444,25 +545,18 @@ int batch_execute(Batch& b, cudaStream_t st, int sms, TileConfig& tile, ExecStat
         if (e != cudaSuccess) return fail("decoder relaunch", e);
         x.launches++;
     }
-    int2* d_best = reinterpret_cast<int2*>(b.d_mem + b.o_best);
-    const InstDesc* d_inst = reinterpret_cast<const InstDesc*>(b.d_mem + b.o_desc);
-    const SlotHead* d_heads = reinterpret_cast<const SlotHead*>(b.d_mem + b.o_heads);
-    e = launch_select_best(d_inst, (int)b.desc.size(), d_heads, d_best, st);
-    if (e != cudaSuccess) return fail("select launch", e);
-    x.launches++;
-    if (b.best_only) {
-        unsigned long long* d_g = reinterpret_cast<unsigned long long*>(b.d_mem + b.o_gather);
-        e = launch_gather_best(d_inst, (int)b.desc.size(), d_best,
-                               reinterpret_cast<const unsigned long long*>(b.d_mem + b.o_places), d_g,
-                               b.max_stride, st);
-        if (e != cudaSuccess) return fail("gather launch", e);
-        x.launches++;
+    {
+        int n = 0;
+        e = enqueue_select(b, st, &n);
+        x.launches += n;
+        if (e != cudaSuccess) return fail("select launch", e);
     }
     e = cudaEventRecord(b.ev[2], st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return fail("select", e);
     cudaEventElapsedTime(&ms, b.ev[0], b.ev[2]);
     x.device_ms = ms;
+    if (graph && !retried) batch_capture(b, st, sms, t);
     tile = t;
     if (xs) *xs = x;
     return PLP_OK;
@@ -509,7 +603,7 @@ size_t batch_d2h_bytes(const Batch& b) {
 int run_batch(Batch& b, cudaStream_t st, Pinned& pin, int sms, TileConfig& tile) {
     int s = batch_prepare(b, st, pin, sms, tile);
     if (s != PLP_OK) return s;
-    s = batch_execute(b, st, sms, tile, nullptr);
+    s = batch_execute(b, st, sms, tile, nullptr, false);
     if (s != PLP_OK) return s;
     s = batch_fetch(b, st);
     if (s != PLP_OK) return s;
@@ -1027,6 +1121,99 @@ int plp_set_tile(plp_handle* h, int32_t P, int32_t C, int32_t G, int32_t D, int3
     return PLP_OK;
 }
 
+int plp_autotune(plp_handle* h, const plp_instance* const* insts, int32_t n_inst, const plp_run_opts* opts,
+                 int32_t n_opts, int32_t max_decodes, int32_t* tile_out) {
+    if (!h || !insts || !opts || n_inst < 1 || (n_opts != 1 && n_opts != n_inst) || max_decodes < 0) {
+        int s = set_error(PLP_E_INVALID, "plp_autotune: bad argument");
+        record(h, s);
+        return s;
+    }
+    std::vector<const Instance*> in;
+    std::vector<plp_run_opts> op;
+    for (int i = 0; i < n_inst; i++) {
+        if (!insts[i]) {
+            int s = set_error(PLP_E_INVALID, "plp_autotune: null instance");
+            record(h, s);
+            return s;
+        }
+        in.push_back(&insts[i]->inst);
+        op.push_back(opts[n_opts == 1 ? 0 : i]);
+    }
+    std::lock_guard<std::mutex> g(h->sync_mu);
+    cudaSetDevice(h->device);
+    Batch full;
+    int s = full.build(in, op);
+    if (s != PLP_OK) {
+        record(h, s);
+        return s;
+    }
+    // strided sample of the longest-first work list keeps its mix of lengths
+    const size_t n = full.work.size();
+    const size_t m = std::min(n, (size_t)(max_decodes ? max_decodes : 8192));
+    std::vector<int2> sample(m);
+    for (size_t k = 0; k < m; k++) sample[k] = full.work[k * n / m];
+    // candidate tiles: one warp per decoder; depths around the instance sizes
+    int max_steps = 1;
+    for (const auto& d : full.desc) max_steps = std::max(max_steps, d.n_steps);
+    std::vector<int> Ps, Cs;
+    for (int p : {64, 128, 256})
+        if (p <= P_MAX && (p >= std::min(max_steps, 64) || p == 128)) Ps.push_back(p);
+    for (int c : {256, 384, 512, 768}) Cs.push_back(c);
+    const int dm[][2] = {{8, 1}, {8, 2}, {4, 1}, {4, 4}, {2, 1}};
+    std::vector<TileConfig> cand;
+    for (int p : Ps)
+        for (int c : Cs)
+            for (const auto& x : dm) {
+                TileConfig t;
+                t.P = p; t.C = c; t.G = 1; t.D = x[0]; t.M = x[1];
+                fit_tile(t, full.Hz);
+                if (decoder_smem_bytes(t.P, t.C, full.Hz, t.G) * t.D > 227 * 1024) continue;
+                bool dup = false;
+                for (const auto& u : cand) dup = dup || same_tile(u, t);
+                if (!dup) cand.push_back(t);
+            }
+    double best_ms = 1e30;
+    TileConfig best;
+    {
+        std::lock_guard<std::mutex> lk(h->mu);
+        best = h->tile;
+    }
+    for (const TileConfig& t0 : cand) {
+        Batch b;
+        s = b.build(in, op);
+        if (s != PLP_OK) break;
+        b.work = sample;
+        TileConfig t = t0;
+        s = batch_prepare(b, h->sync_stream, h->sync_pin, h->sms, t);
+        if (s != PLP_OK) break;
+        double ms = 1e30;
+        for (int rep = 0; rep < 3 && s == PLP_OK; rep++) {
+            ExecStats x;
+            TileConfig u = t0;
+            s = batch_execute(b, h->sync_stream, h->sms, u, &x, false);
+            if (s == PLP_OK && rep > 0) ms = std::min(ms, x.device_ms);
+        }
+        if (s != PLP_OK) break;   // batch_execute released the batch
+        batch_release(b, h->sync_stream);
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = t0;
+        }
+    }
+    if (s != PLP_OK) {
+        record(h, s);
+        return s;
+    }
+    {
+        std::lock_guard<std::mutex> lk(h->mu);
+        h->tile = best;
+    }
+    if (tile_out) {
+        tile_out[0] = best.P; tile_out[1] = best.C; tile_out[2] = best.G; tile_out[3] = best.D; tile_out[4] = best.M;
+    }
+    return PLP_OK;
+}
+
 int plp_solve(plp_handle* h, const plp_instance* const* insts, int32_t n_inst,
               const plp_run_opts* opts, int32_t n_opts, plp_result** results) {
     if (!h || !insts || !opts || !results || n_inst < 1 || (n_opts != 1 && n_opts != n_inst)) {
@@ -1251,7 +1438,7 @@ int plp_batch_run(plp_batch* pb, double* device_ms, double* decoder_ms, int32_t*
         tile = h->tile;
     }
     ExecStats x;
-    int s = batch_execute(pb->b, h->sync_stream, h->sms, tile, &x);
+    int s = batch_execute(pb->b, h->sync_stream, h->sms, tile, &x, true);
     if (s != PLP_OK) {
         record(h, s);
         return s;
@@ -1290,6 +1477,8 @@ int plp_batch_io_bytes(const plp_batch* pb, int64_t* h2d, int64_t* d2h) {
     if (d2h) *d2h = (int64_t)batch_d2h_bytes(pb->b);
     return PLP_OK;
 }
+
+int plp_batch_graph(const plp_batch* pb) { return pb && pb->b.gexec ? 1 : 0; }
 
 void plp_batch_free(plp_batch* pb) {
     if (!pb) return;

@@ -1658,9 +1658,7 @@ static DecoderFn decoder_fn(int G, int D, int M) {
 
 bool decoder_config_supported(int G, int D, int M) { return decoder_fn(G, D, M) != nullptr; }
 
-cudaError_t launch_decoder(const DecodeLaunch& L, cudaStream_t st) {
-    DecoderFn fn = decoder_fn(L.warps_per_decoder, L.decoders_per_cta, L.min_blocks);
-    if (!fn) return cudaErrorInvalidConfiguration;
+static DecoderArgs decoder_args(const DecodeLaunch& L) {
     DecoderArgs a;
     a.inst = L.inst;
     a.step_type = L.step_type;
@@ -1677,15 +1675,37 @@ cudaError_t launch_decoder(const DecodeLaunch& L, cudaStream_t st) {
     a.P = L.P;
     a.C = L.C;
     a.Hz = L.Hz;
-    const int smem = decoder_smem_bytes(L.P, L.C, L.Hz, L.warps_per_decoder) * L.decoders_per_cta;
-    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    if (e != cudaSuccess) return e;
-    e = cudaMemsetAsync(L.work_next, 0, sizeof(int), st);
+    return a;
+}
+
+static int decoder_launch_smem(const DecodeLaunch& L) {
+    return decoder_smem_bytes(L.P, L.C, L.Hz, L.warps_per_decoder) * L.decoders_per_cta;
+}
+
+// Function attributes (dynamic shared memory) for a launch; not a stream
+// operation, so it is done before any capture.
+cudaError_t configure_decoder(const DecodeLaunch& L) {
+    DecoderFn fn = decoder_fn(L.warps_per_decoder, L.decoders_per_cta, L.min_blocks);
+    if (!fn) return cudaErrorInvalidConfiguration;
+    return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, decoder_launch_smem(L));
+}
+
+// Stream operations only (counter resets and the launch): capturable.
+cudaError_t enqueue_decoder(const DecodeLaunch& L, cudaStream_t st) {
+    DecoderFn fn = decoder_fn(L.warps_per_decoder, L.decoders_per_cta, L.min_blocks);
+    if (!fn) return cudaErrorInvalidConfiguration;
+    cudaError_t e = cudaMemsetAsync(L.work_next, 0, sizeof(int), st);
     if (e != cudaSuccess) return e;
     e = cudaMemsetAsync(L.abort, 0, sizeof(int), st);
     if (e != cudaSuccess) return e;
-    fn<<<L.ctas, 32 * L.warps_per_decoder * L.decoders_per_cta, smem, st>>>(a);
+    fn<<<L.ctas, 32 * L.warps_per_decoder * L.decoders_per_cta, decoder_launch_smem(L), st>>>(decoder_args(L));
     return cudaGetLastError();
+}
+
+cudaError_t launch_decoder(const DecodeLaunch& L, cudaStream_t st) {
+    cudaError_t e = configure_decoder(L);
+    if (e != cudaSuccess) return e;
+    return enqueue_decoder(L, st);
 }
 
 cudaError_t decoder_occupancy(int P, int C, int Hz, int G, int D, int M, int* ctas_per_sm) {

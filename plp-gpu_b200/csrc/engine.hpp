@@ -31,7 +31,9 @@ struct DecodeLaunch {
 int decoder_smem_bytes(int P, int C, int Hz, int G);
 bool decoder_config_supported(int G, int D, int M);
 cudaError_t decoder_occupancy(int P, int C, int Hz, int G, int D, int M, int* ctas_per_sm);
-cudaError_t launch_decoder(const DecodeLaunch& L, cudaStream_t st);
+cudaError_t launch_decoder(const DecodeLaunch& L, cudaStream_t st);     // configure + enqueue
+cudaError_t configure_decoder(const DecodeLaunch& L);                    // function attributes
+cudaError_t enqueue_decoder(const DecodeLaunch& L, cudaStream_t st);     // stream operations only
 cudaError_t launch_select_best(const InstDesc* inst, int n_inst, const SlotHead* heads, int2* best,
                                cudaStream_t st);
 cudaError_t launch_rng_dump(const long long* seeds, int n_seeds, int n_random, int n_bits,

@@ -100,6 +100,8 @@ def lib():
         "plp_create": (ctypes.c_int, [SZ, I32, P]),
         "plp_destroy": (None, [P]),
         "plp_set_tile": (ctypes.c_int, [P, I32, I32, I32, I32, I32]),
+        "plp_autotune": (ctypes.c_int, [P, P, I32, P, I32, I32, P]),
+        "plp_batch_graph": (ctypes.c_int, [P]),
         "plp_solve": (ctypes.c_int, [P, P, I32, P, I32, P]),
         "plp_submit": (ctypes.c_int, [P, P, P, P]),
         "plp_poll": (ctypes.c_int, [P, I64]),
@@ -326,6 +328,15 @@ class Handle:
     def set_tile(self, P: int = 0, C: int = 0, G: int = 0, D: int = 0, M: int = 0):
         _check(lib().plp_set_tile(self._p, P, C, G, D, M), self._p)
 
+    def autotune(self, instances, opts, max_decodes: int = 0) -> tuple:
+        """Times candidate tiles on a sample of the workload and keeps the
+        fastest for later solves; returns (P, C, G, D, M)."""
+        insts = (ctypes.c_void_p * len(instances))(*[i._p.value for i in instances])
+        oarr = (RunOpts * 1)(opts) if isinstance(opts, RunOpts) else (RunOpts * len(opts))(*opts)
+        out = (ctypes.c_int32 * 5)()
+        _check(lib().plp_autotune(self._p, insts, len(instances), oarr, len(oarr), max_decodes, out), self._p)
+        return tuple(out)
+
     def solve(self, instances, opts) -> list:
         """opts: one RunOpts for all instances or a list with one per instance."""
         insts = (ctypes.c_void_p * len(instances))(*[i._p.value for i in instances])
@@ -383,6 +394,11 @@ class Batch:
         dm, km, nl = ctypes.c_double(), ctypes.c_double(), ctypes.c_int32()
         _check(lib().plp_batch_run(self._p, ctypes.byref(dm), ctypes.byref(km), ctypes.byref(nl)), self._h._p)
         return dm.value, km.value, nl.value
+
+    @property
+    def graph(self) -> bool:
+        """True when the next run replays the batch's captured CUDA graph."""
+        return bool(lib().plp_batch_graph(self._p))
 
     def fetch(self) -> list:
         res = (ctypes.c_void_p * self._n)()

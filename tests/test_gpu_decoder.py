@@ -142,3 +142,44 @@ def test_reference_work_accounting_matches_oracle_counter(handle):
         for k in range(seeds):
             _, _, _, st = O.run(oi, seed=11 + k, stats=True)
             assert r.work(k) == (st["aabb_full"], st["pairs"])
+
+
+def test_graph_replay_gives_identical_results():
+    inst = P.Instance.parse(synth.multi_restart(2).to_thpack())
+    with P.Handle() as h:
+        b = h.prepare([inst], P.make_opts(seed=3, restarts=96))
+        assert not b.graph
+        b.run()
+        first = [O.strip_time(b.fetch()[0].json(k)) for k in range(96)]
+        assert b.graph                      # the clean run was captured
+        for _ in range(2):
+            dm, km, nl = b.run()            # graph replays
+            assert nl == 2 and dm >= km > 0
+            again = [O.strip_time(b.fetch()[0].json(k)) for k in range(96)]
+            assert again == first
+        b.close()
+
+
+def test_graph_replay_best_only_gather():
+    insts = [P.Instance.parse(i.to_thpack()) for i in synth.batched_set(6, 31000)]
+    with P.Handle() as h:
+        direct = [r.json(r.best()[0]) for r in h.solve(insts, P.make_opts(seed=1, restarts=24))]
+        b = h.prepare(insts, P.make_opts(seed=1, restarts=24, best_only=True))
+        b.run()
+        b.run()
+        assert b.graph
+        res = b.fetch()
+        assert [O.strip_time(r.json(r.best()[0])) for r in res] == [O.strip_time(j) for j in direct]
+        b.close()
+
+
+def test_autotune_picks_a_supported_tile_and_keeps_results():
+    insts = [P.Instance.parse(i.to_thpack()) for i in synth.batched_set(8, 32000)]
+    opts = P.make_opts(seed=2, restarts=32)
+    with P.Handle() as h:
+        before = [[O.strip_time(r.json(k)) for k in range(r.restarts)] for r in h.solve(insts, opts)]
+        tile = h.autotune(insts, opts, max_decodes=128)
+        Pd, Cd, G, D, M = tile
+        assert G == 1 and (G, D, M) in CONFIGS and Pd >= 32 and Cd % 32 == 0
+        after = [[O.strip_time(r.json(k)) for k in range(r.restarts)] for r in h.solve(insts, opts)]
+        assert after == before
