@@ -262,6 +262,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--tile", default=None,
+                    help="P,C,G,D,M decoder tile instead of the autotuner's choice (profiling runs)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -297,10 +299,18 @@ def main():
     h = P.Handle(device=local)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")   # > 126 MB L2
 
+    # ---- tile: the project's autotuner, on a sample of this workload ----
+    if args.tile:
+        tile = tuple(int(v) for v in args.tile.split(","))
+        h.set_tile(*tile)
+    else:
+        tile = h.autotune(insts, opts, max_decodes=8192)
+
     # ---- device-resident timing (value) ----
     batch = h.prepare(insts, opts)
     for _ in range(args.warmup):
         batch.run()
+    graph = batch.graph          # later runs replay one captured CUDA graph
     warm_results = batch.fetch()
     parity = golden_parity(warm_results, opts.seed, args.workload)
     # algorithmic work of the reference per decode (replayed from the results)
@@ -354,7 +364,14 @@ def main():
                            "(sm_max_mhz of MEASURED_PEAKS.json)",
             "work_unit": f"reference AABB tests per decode T = {t_mean:.0f} (mean over the step's "
                          f"restarts) x {INT_OPS_PER_AABB} int ops",
-            "kernel": "decoder_kernel", "kernel_ms_per_launch": dec_mean_ms,
+            "issue_active_pct_ncu": float(prof[f"issue_active_pct.{args.workload}"])
+            if f"issue_active_pct.{args.workload}" in prof else None,
+            "fp64_pipe_pct_ncu": float(prof[f"fp64_pipe_pct.{args.workload}"])
+            if f"fp64_pipe_pct.{args.workload}" in prof else None,
+            "note": "T counts the reference's full C1/C3 scans; the incremental decoder skips most of "
+                    "them, so frac can exceed 1. issue_active_pct_ncu is the hardware's own measure.",
+            "kernel": "decoder1_kernel" if tile[2] == 1 else "decoder_kernel",
+            "kernel_ms_per_launch": dec_mean_ms,
         }
         cpu = None
         if not args.no_cpu_baseline:
@@ -388,7 +405,8 @@ def main():
                        "items_per_instance": [min(n_items), max(n_items)],
                        "parallelism": f"dp{world} (restarts sharded by rank)",
                        "l2": "flushed between timed steps (256 MiB write)",
-                       "tile_after_warmup": None},
+                       "tile": dict(zip(("P", "C", "G", "D", "M"), tile)), "tile_source": "--tile" if args.tile else "plp_autotune",
+                       "cuda_graph": graph},
             "parity": parity,
             "e2e": {"value": e2e_value, "unit": "decodes/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},

@@ -12,12 +12,19 @@
 //   selection          plp/solver.py:156-166, gpu/plp_common.hpp:493-511
 //   rows               gpu/plp_gpu.cu:350 (restart k = PyRng(seed + k))
 //
-// Layout of one decoder (a warp) in shared memory:
+// Two persistent decoders share the work list and result layout:
+//   decoder1_kernel<D, M>    one warp per restart, incremental per-point
+//                            evaluation (the default; see its section)
+//   decoder_kernel<G, D, M>  G warps per restart, lockstep scan of the
+//                            filtered points every step (multi-warp variant)
+//
+// Layout of one decoder in shared memory (both kernels):
 //   MT19937 state       624 x u32
 //   placed boxes        sorted by top z (ascending): {x, y, x2, y2} int4,
 //                       bottom z, top z, placement index
-//   live points         sorted unique keys (z, y, x), double buffer
-//   point masks         one byte per live point (random branch)
+//   live points         sorted unique keys (z, y, x) (+ per-point state and
+//                       contact areas in decoder1_kernel)
+//   item list           the points to evaluate this step
 // FSR reuses the point buffers as scratch once the pass is done.
 //
 // Exactness notes (why the device results equal the reference's):
@@ -29,10 +36,11 @@
 //    same when they are dropped. The live list is exactly the reference's
 //    candidate set minus covered points, in the same (z, y, x) order.
 //  * C1/C2/C3 are evaluated per point for all orientations at once. C2 is the
-//    same integer test; C3 sums the same integer overlap areas and keeps the
-//    reference's FP64 ratio test (double)s / (double)(w*d) < 0.5; C1 only
-//    visits boxes whose top lies above z (a box with top <= z cannot overlap
-//    a box starting at z), which does not change the boolean.
+//    same integer test; C3 sums the same integer overlap areas (the ratio
+//    test is the reference's FP64 form in decoder_kernel and its exact
+//    integer equivalent in decoder1_kernel); C1 only visits boxes whose top
+//    lies above z (a box with top <= z cannot overlap a box starting at z),
+//    which does not change the boolean.
 //  * The first feasible pair (greedy branch) is found by scanning points in
 //    order; random() is drawn only after one feasible pair exists, and the
 //    full count / idx-th selection runs only on the random branch.
