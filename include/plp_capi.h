@@ -104,14 +104,18 @@ void plp_free(void* p);
 typedef struct {
     int64_t seed;         /* restart k uses PyRng(|seed + k|) */
     int32_t restarts;     /* >= 1 */
-    int32_t passes;       /* >= 1 fixed passes per restart (RNG carried over) */
+    int32_t passes;       /* >= 1 fixed passes per restart (RNG carried over); with a
+                             time limit, the most passes to run (0 = no cap) */
     double eps;           /* eps-greedy probability */
     double theta;         /* acceptance threshold; NaN = no threshold (--no-theta) */
     int32_t order;        /* 0 = volume, 1 = input */
     int32_t first_fit;    /* 1 = always the first feasible pair */
     double mu;            /* friction coefficient (reference default 0.2) */
-    double time_limit_s;  /* < 0: exactly `passes` passes; >= 0: passes until the
-                             wall clock reaches it (plp_run_plain only) */
+    double time_limit_s;  /* < 0: exactly `passes` passes; >= 0: passes until this
+                             much time has passed since the restart began (at
+                             least one; gpu/plp_common.hpp:484-492). The device
+                             decoders read the GPU's global timer after each pass;
+                             the summary's n_passes is the count run. */
     int32_t best_only;    /* 1: copy back the placements of the best restart only
                              (summaries of every restart are always returned) */
 } plp_run_opts;

@@ -162,8 +162,9 @@ struct Batch {
         for (size_t i = 0; i < in.size(); i++) {
             const Instance& I = *in[i];
             const plp_run_opts& o = op[i];
-            if (o.restarts < 1 || o.passes < 1)
-                return set_error(PLP_E_INVALID, "restarts and passes must be >= 1");
+            const bool budget = o.time_limit_s >= 0;   // wall-clock budget, passes = cap (0: none)
+            if (o.restarts < 1 || o.passes < 0 || (!budget && o.passes < 1))
+                return set_error(PLP_E_INVALID, "restarts must be >= 1 and passes >= 1 (>= 0 with a time limit)");
             if (o.order != 0 && o.order != 1) return set_error(PLP_E_INVALID, "order must be 0 or 1");
             int xb = 0, yb = 0, zb = 0;
             for (int v = I.L; v; v >>= 1) xb++;
@@ -185,7 +186,8 @@ struct Batch {
             d.restarts = o.restarts;
             d.slot_base = (int)n_slots;
             d.place_stride = std::max(1, d.n_steps);
-            d.passes = o.passes;
+            d.passes = budget && o.passes == 0 ? INT_MAX : o.passes;
+            d.budget_ns = budget ? (long long)std::min(o.time_limit_s * 1e9, 9.0e18) : -1;
             d.place_off = n_places;
             d.seed = o.seed;
             d.eps = o.eps;
@@ -209,7 +211,7 @@ struct Batch {
             n_places += (long long)o.restarts * d.place_stride;
             max_stride = std::max(max_stride, d.place_stride);
             max_steps = std::max(max_steps, d.n_steps);
-            multi_pass = multi_pass || o.passes > 1;
+            multi_pass = multi_pass || d.passes > 1;
             best_only = best_only && o.best_only;
             maxH = std::max(maxH, I.H);
         }
@@ -220,7 +222,8 @@ struct Batch {
         std::vector<int> order(in.size());
         for (size_t i = 0; i < in.size(); i++) order[i] = (int)i;
         std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
-            return desc[a].n_steps * desc[a].passes > desc[b].n_steps * desc[b].passes;
+            return (long long)desc[a].n_steps * std::min(desc[a].passes, 1 << 16) >
+                   (long long)desc[b].n_steps * std::min(desc[b].passes, 1 << 16);
         });
         work.reserve(n_slots);
         for (int i : order)
@@ -706,7 +709,7 @@ size_t request_bytes(const Instance& I, const plp_run_opts& o) {
     const size_t steps = (size_t)std::max(1, I.n_items());
     return 4096 + I.types.size() * sizeof(TypeOrs) + steps * 4 +
            (size_t)o.restarts * (sizeof(int2) + sizeof(SlotHead) + steps * 8) +
-           (o.passes > 1 ? (size_t)148 * 64 * steps * 8 : 0);
+           (o.passes > 1 || (o.time_limit_s >= 0 && o.passes == 0) ? (size_t)148 * 64 * steps * 8 : 0);
 }
 
 void worker_main(plp_handle* h, int wi) {
@@ -1262,7 +1265,8 @@ int plp_submit(plp_handle* h, const plp_instance* inst, const plp_run_opts* opts
         record(h, s);
         return s;
     }
-    if (opts->restarts < 1 || opts->passes < 1 || (opts->order != 0 && opts->order != 1)) {
+    if (opts->restarts < 1 || opts->passes < 0 || (opts->time_limit_s < 0 && opts->passes < 1) ||
+        (opts->order != 0 && opts->order != 1)) {
         int s = set_error(PLP_E_INVALID, "plp_submit: bad options");
         record(h, s);
         return s;

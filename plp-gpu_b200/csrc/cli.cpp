@@ -7,12 +7,14 @@
 //   plp_gpu --selftest | --rngdump N
 //
 // Modes:
-//   --single-pass or --passes N   persistent device decoder, one restart
+//   --single-pass or --passes N   persistent device decoder, fixed pass count
+//   neither (wall-clock budget)   persistent device decoder, passes until
+//                                 --time has elapsed for the restart (the
+//                                 decoder reads the GPU's global timer)
 //   --batch K / --device K        K restarts (row k = seed + k) in one launch;
 //                                 JSON wrapper {"K", "n_passes", "time_s", "rows"}
-//   neither (wall-clock budget)   host pass loop with one device feasibility
-//                                 launch per item step, until --time elapses
-//   --plain                       force the per-step path for fixed passes too
+//   --plain                       the per-step path instead: host pass loop
+//                                 with one device feasibility launch per step
 // Exit codes: 0 ok; 1 instance error, CUDA error or device error; 2 usage.
 #include <cmath>
 #include <cstdio>
@@ -172,11 +174,11 @@ int main(int argc, char** argv) {
     o.first_fit = first_fit ? 1 : 0;
     o.mu = mu;
     const bool fixed = single || passes > 0;
-    o.passes = single ? 1 : (passes > 0 ? passes : 1);
+    o.passes = single ? 1 : (passes > 0 ? passes : 0);   // 0: no cap under --time
     o.time_limit_s = fixed ? -1.0 : time_s;
     plp_result* res = nullptr;
     int st;
-    if (plain || !fixed) {
+    if (plain) {
         st = plp_run_plain(inst, &o, &res);
     } else {
         plp_handle* h = nullptr;

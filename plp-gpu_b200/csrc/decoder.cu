@@ -64,7 +64,7 @@ struct DecShared {
     unsigned long long bar;   // mbarrier of the decoder's warps (G > 1)
     int item;      // current work item
     int nW;        // items in the filtered point list
-    int wnext;     // next unclaimed item
+    int wnext;     // multi-warp decoder: warp 0's end-of-pass-loop decision
     int best_w;    // smallest feasible item found so far
     int full;      // random branch: every feasible pair is needed
     int err;
@@ -684,6 +684,8 @@ __device__ __forceinline__ void decoder_body(const DecoderArgs& a, unsigned char
             const long long sd = I.seed + restart;
             mt_seed_warp(mt, (unsigned long long)(sd < 0 ? -sd : sd), a.mt_init, lane);
         }
+        const long long t0 = global_ns();   // read by warp 0 only
+        int npass = 0;
         int err = ERR_NONE;
         bool have_acc = false, have_any = false;
         long long best_vol = 0;
@@ -827,9 +829,16 @@ __device__ __forceinline__ void decoder_body(const DecoderArgs& a, unsigned char
                 }
                 have_any = true;
                 have_acc = have_acc || acc;
+                // wall-clock budget (gpu/plp_common.hpp:484-492), decided by warp 0
+                const bool stop = I.budget_ns >= 0 && __shfl_sync(FULL, global_ns() - t0, 0) >= I.budget_ns;
+                if (lane == 0) sh->wnext = stop ? 1 : 0;
                 __syncwarp();
             }
             PLP_SYNC()   // FSR scratch overlays the point buffers
+            npass = pass + 1;
+            const bool stop = sh->wnext != 0;
+            PLP_SYNC()   // every warp has read the decision
+            if (stop) break;
         }
         if (g == 0 && lane == 0) {
             if (err) atomicOr(a.err_flag, 1 << err);
@@ -838,7 +847,7 @@ __device__ __forceinline__ void decoder_body(const DecoderArgs& a, unsigned char
             h.err = err;
             h.volume = err ? 0 : best_vol;
             h.score = err ? 0.0 : best_score;
-            h.n_passes = I.passes;
+            h.n_passes = npass;
             h.fallback = have_acc ? 0 : 1;
             a.heads[slot] = h;
         }
@@ -1300,6 +1309,8 @@ __device__ __forceinline__ void decoder1_body(const DecoderArgs& a, unsigned cha
             const long long sd = I.seed + restart;
             mt_seed_warp(mt, (unsigned long long)(sd < 0 ? -sd : sd), a.mt_init, lane);
         }
+        const long long t0 = global_ns();   // the reference's run() clock starts after seeding
+        int npass = 0;
         int err = ERR_NONE;
         bool have_acc = false, have_any = false;
         long long best_vol = 0;
@@ -1438,7 +1449,10 @@ __device__ __forceinline__ void decoder1_body(const DecoderArgs& a, unsigned cha
             }
             have_any = true;
             have_acc = have_acc || acc;
+            npass = pass + 1;
             __syncwarp();
+            // wall-clock budget (gpu/plp_common.hpp:484-492): stop once it is spent
+            if (I.budget_ns >= 0 && __shfl_sync(FULL, global_ns() - t0, 0) >= I.budget_ns) break;
         }
         if (lane == 0) {
             if (err) atomicOr(a.err_flag, 1 << err);
@@ -1447,7 +1461,7 @@ __device__ __forceinline__ void decoder1_body(const DecoderArgs& a, unsigned cha
             h.err = err;
             h.volume = err ? 0 : best_vol;
             h.score = err ? 0.0 : best_score;
-            h.n_passes = I.passes;
+            h.n_passes = npass;
             h.fallback = have_acc ? 0 : 1;
             a.heads[slot] = h;
         }

@@ -29,7 +29,16 @@ struct InstDesc {
     long long seed;      // restart k is seeded with |seed + k|
     double eps, theta, mu;
     int has_theta, first_fit;
+    long long budget_ns; // >= 0: passes (at most `passes`) until this much
+                         // global-timer time has passed since the restart began
 };
+
+// Nanoseconds of the GPU's global timer (one clock for all SMs).
+__device__ __forceinline__ long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return (long long)t;
+}
 
 // Orientation table entry of one box type: up to 6 (w, d, h), dedup'd in the
 // reference's parser order (gpu/plp_common.hpp:269-280); unused slots are 0.

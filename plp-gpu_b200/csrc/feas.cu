@@ -322,7 +322,9 @@ int run_plain(const Instance& inst, const plp_run_opts& o, std::vector<RunSummar
             }
             have_any = true;
             have_acc = have_acc || acc;
-            const bool done = o.time_limit_s < 0 ? k >= o.passes : now_seconds() - t0 >= o.time_limit_s;
+            const bool done = o.time_limit_s < 0
+                                  ? k >= o.passes
+                                  : now_seconds() - t0 >= o.time_limit_s || (o.passes > 0 && k >= o.passes);
             if (done) break;
         }
         RunSummary& S = summ[r];

@@ -125,3 +125,18 @@ def test_reference_decoder_on_capi_backend_matches_reference_host():
                                  text=True, check=True, timeout=600)
             assert _strip(out.stdout) == _ref([f.name, "--single-pass", "--json"] + flags)
         os.unlink(f.name)
+
+
+@pytest.mark.gpu
+def test_time_budget_on_device_equals_fixed_passes(inst_file):
+    """--time S without --single-pass runs passes on the device until S has
+    elapsed (the reference's run loop); the packing equals a fixed run of the
+    pass count it reports."""
+    r = run([inst_file, "--time", "0.01", "--seed", "3", "--json"])
+    assert r.returncode == 0, r.stderr
+    d = _strip(r.stdout)
+    n = d["n_passes"]
+    assert n >= 2
+    fixed = run([inst_file, "--passes", str(n), "--seed", "3", "--json"])
+    assert fixed.returncode == 0
+    assert _strip(fixed.stdout) == d

@@ -183,3 +183,39 @@ def test_autotune_picks_a_supported_tile_and_keeps_results():
         assert G == 1 and (G, D, M) in CONFIGS and Pd >= 32 and Cd % 32 == 0
         after = [[O.strip_time(r.json(k)) for k in range(r.restarts)] for r in h.solve(insts, opts)]
         assert after == before
+
+
+def _jsons(res):
+    return [O.strip_time(res.json(k)) for k in range(res.restarts)]
+
+
+def test_time_budget_zero_runs_exactly_one_pass():
+    inst = P.Instance.parse(synth.multi_restart(2).to_thpack())
+    with P.Handle() as h:
+        r = h.solve([inst], P.make_opts(seed=5, restarts=16, passes=0, time_limit_s=0.0))[0]
+        one = h.solve([inst], P.make_opts(seed=5, restarts=16, passes=1))[0]
+    assert all(r.summary(k).n_passes == 1 for k in range(16))
+    assert _jsons(r) == _jsons(one)
+
+
+def test_time_budget_matches_fixed_pass_count_and_oracle():
+    text = synth.single_pass(1).to_thpack()
+    inst = P.Instance.parse(text)
+    with P.Handle() as h:
+        r = h.solve([inst], P.make_opts(seed=7, restarts=6, passes=0, time_limit_s=0.01))[0]
+        counts = [r.summary(k).n_passes for k in range(6)]
+        assert min(counts) >= 2
+        for k in range(6):
+            f = h.solve([inst], P.make_opts(seed=7 + k, restarts=1, passes=counts[k]))[0]
+            assert O.strip_time(r.json(k)) == O.strip_time(f.json(0))
+    js, _, _ = O.run(O.OInstance(text), seed=7, passes=counts[0])
+    assert O.strip_time(r.json(0)) == O.strip_time(js)
+
+
+def test_time_budget_pass_cap_binds():
+    inst = P.Instance.parse(synth.single_pass(1).to_thpack())
+    with P.Handle() as h:
+        r = h.solve([inst], P.make_opts(seed=1, restarts=8, passes=3, time_limit_s=30.0))[0]
+        f = h.solve([inst], P.make_opts(seed=1, restarts=8, passes=3))[0]
+    assert [r.summary(k).n_passes for k in range(8)] == [3] * 8
+    assert _jsons(r) == _jsons(f)
