@@ -3,7 +3,7 @@
 //
 //   plp_gpu <instance> [--seed N] [--time S] [--eps F] [--theta F | --no-theta]
 //           [--order volume|input] [--first-fit] [--mu F] [--single-pass] [--json]
-//           [--batch K | --device K] [--passes N] [--plain]
+//           [--batch K | --device K] [--passes N] [--plain] [--multi]
 //   plp_gpu --selftest | --rngdump N
 //
 // Modes:
@@ -15,8 +15,15 @@
 //                                 JSON wrapper {"K", "n_passes", "time_s", "rows"}
 //   --plain                       the per-step path instead: host pass loop
 //                                 with one device feasibility launch per step
+//   --multi                       accept a file with P >= 1 instances (the
+//                                 reference rejects P > 1) and solve all of
+//                                 them in one batched launch; one output line
+//                                 per instance, in file order
 // Exit codes: 0 ok; 1 instance error, CUDA error or device error; 2 usage.
 #include <cmath>
+#include <fstream>
+#include <sstream>
+#include <vector>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -31,7 +38,7 @@ void usage(const char* prog) {
     std::fprintf(stderr,
                  "usage: %s <instance> [--seed N] [--time S] [--eps F] [--theta F | --no-theta]\n"
                  "                 [--order volume|input] [--first-fit] [--mu F] [--single-pass]\n"
-                 "                 [--batch K | --device K] [--passes N] [--plain] [--json]\n"
+                 "                 [--batch K | --device K] [--passes N] [--plain] [--multi] [--json]\n"
                  "       %s --selftest | --rngdump N\n",
                  prog, prog);
 }
@@ -95,7 +102,7 @@ int main(int argc, char** argv) {
     std::string path, order = "volume";
     long long seed = 0;
     double time_s = 300.0, eps = 0.3, theta = 0.9, mu = 0.2;
-    bool no_theta = false, first_fit = false, single = false, as_json = false, plain = false;
+    bool no_theta = false, first_fit = false, single = false, as_json = false, plain = false, multi = false;
     int batch = 0, device = 0, passes = 0;
     if (const char* e = std::getenv("PLP_MU")) mu = std::strtod(e, nullptr);
     for (int i = 1; i < argc; i++) {
@@ -129,6 +136,7 @@ int main(int argc, char** argv) {
         else if (a == "--device") device = std::atoi(next("--device").c_str());
         else if (a == "--passes") passes = std::atoi(next("--passes").c_str());
         else if (a == "--plain") plain = true;
+        else if (a == "--multi") multi = true;
         else if (a == "-h" || a == "--help") { usage(argv[0]); return 0; }
         else if (!a.empty() && a[0] != '-') {
             if (!path.empty()) { usage(argv[0]); return 2; }
@@ -140,14 +148,39 @@ int main(int argc, char** argv) {
         }
     }
     if (path.empty()) { usage(argv[0]); return 2; }
-    plp_instance* inst = nullptr;
-    if (plp_instance_load(path.c_str(), &inst) != PLP_OK) {
-        std::fprintf(stderr, "instance error: %s\n", plp_last_error(nullptr));
-        return 1;
+    std::vector<plp_instance*> insts;
+    if (multi) {
+        std::ifstream f(path, std::ios::binary);
+        if (!f) {
+            std::fprintf(stderr, "instance error: cannot open %s\n", path.c_str());
+            return 1;
+        }
+        std::ostringstream ss;
+        ss << f.rdbuf();
+        const std::string text = ss.str();
+        plp_instance** arr = nullptr;
+        int32_t n = 0;
+        if (plp_instance_parse_multi(text.data(), text.size(), &arr, &n) != PLP_OK) {
+            std::fprintf(stderr, "instance error: %s\n", plp_last_error(nullptr));
+            return 1;
+        }
+        insts.assign(arr, arr + n);
+        plp_free(arr);
+    } else {
+        plp_instance* one = nullptr;
+        if (plp_instance_load(path.c_str(), &one) != PLP_OK) {
+            std::fprintf(stderr, "instance error: %s\n", plp_last_error(nullptr));
+            return 1;
+        }
+        insts.push_back(one);
     }
+    auto free_insts = [&]() {
+        for (plp_instance* i : insts) plp_instance_free(i);
+        insts.clear();
+    };
     if (order != "volume" && order != "input") {
         std::fprintf(stderr, "unknown order %s\n", order.c_str());
-        plp_instance_free(inst);
+        free_insts();
         return 2;
     }
     if (batch && device) {
@@ -176,51 +209,60 @@ int main(int argc, char** argv) {
     const bool fixed = single || passes > 0;
     o.passes = single ? 1 : (passes > 0 ? passes : 0);   // 0: no cap under --time
     o.time_limit_s = fixed ? -1.0 : time_s;
-    plp_result* res = nullptr;
-    int st;
+    const int n_inst = (int)insts.size();
+    std::vector<plp_result*> res(n_inst, nullptr);
+    int st = PLP_OK;
     if (plain) {
-        st = plp_run_plain(inst, &o, &res);
+        for (int i = 0; i < n_inst && st == PLP_OK; i++) st = plp_run_plain(insts[i], &o, &res[i]);
     } else {
         plp_handle* h = nullptr;
         st = plp_create(0, 0, &h);
         if (st == PLP_OK) {
-            const plp_instance* one = inst;
-            st = plp_solve(h, &one, 1, &o, 1, &res);
+            st = plp_solve(h, insts.data(), n_inst, &o, 1, res.data());
             if (st != PLP_OK) std::fprintf(stderr, "solve: %s\n", plp_last_error(h));
             plp_destroy(h);
         }
     }
-    plp_instance_free(inst);
+    free_insts();
+    auto free_res = [&]() {
+        for (plp_result* r : res)
+            if (r) plp_result_free(r);
+    };
     if (st != PLP_OK) {
         std::fprintf(stderr, "error: %s\n", plp_last_error(nullptr));
+        free_res();
         return 1;
     }
-    for (int k = 0; k < plp_result_restarts(res); k++) {
-        plp_summary s;
-        plp_result_summary(res, k, &s);
-        if (s.err) {
-            std::fprintf(stderr, "device decode error flag %d\n", s.err);
-            plp_result_free(res);
-            return 1;
+    for (plp_result* r : res) {
+        for (int k = 0; k < plp_result_restarts(r); k++) {
+            plp_summary s;
+            plp_result_summary(r, k, &s);
+            if (s.err) {
+                std::fprintf(stderr, "device decode error flag %d\n", s.err);
+                free_res();
+                return 1;
+            }
         }
     }
-    if (K) {
-        plp_summary s0;
-        plp_result_summary(res, 0, &s0);
-        std::printf("{\"K\": %d, \"n_passes\": %d, \"time_s\": %s, \"rows\": [", K, s0.n_passes,
-                    repr(s0.time_s).c_str());
-        for (int k = 0; k < K; k++) std::printf("%s%s", k ? ", " : "", json_of(res, k).c_str());
-        std::printf("]}\n");
-    } else if (as_json) {
-        std::printf("%s\n", json_of(res, 0).c_str());
-    } else {
-        plp_summary s;
-        plp_result_summary(res, 0, &s);
-        std::printf("n_boxes=%d volume_cm3=%lld stability_score=%.4f fallback=%s n_passes=%d "
-                    "time_s=%.3f\n",
-                    s.n_boxes, (long long)s.volume, s.score, s.fallback ? "true" : "false",
-                    s.n_passes, s.time_s);
+    for (plp_result* r : res) {
+        if (K) {
+            plp_summary s0;
+            plp_result_summary(r, 0, &s0);
+            std::printf("{\"K\": %d, \"n_passes\": %d, \"time_s\": %s, \"rows\": [", K, s0.n_passes,
+                        repr(s0.time_s).c_str());
+            for (int k = 0; k < K; k++) std::printf("%s%s", k ? ", " : "", json_of(r, k).c_str());
+            std::printf("]}\n");
+        } else if (as_json) {
+            std::printf("%s\n", json_of(r, 0).c_str());
+        } else {
+            plp_summary s;
+            plp_result_summary(r, 0, &s);
+            std::printf("n_boxes=%d volume_cm3=%lld stability_score=%.4f fallback=%s n_passes=%d "
+                        "time_s=%.3f\n",
+                        s.n_boxes, (long long)s.volume, s.score, s.fallback ? "true" : "false",
+                        s.n_passes, s.time_s);
+        }
     }
-    plp_result_free(res);
+    free_res();
     return 0;
 }

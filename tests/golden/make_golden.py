@@ -97,6 +97,14 @@ CASES = [
     ("stress", lambda: synth.stress_set(2), [0, 1, 2, 3], 1, []),
 ]
 
+# A seeded 1 % sample of the instances of the bench's batched (4096 instances,
+# seeds 30000 + i) and stress (512 instances, seeds 40000 + i) workloads,
+# restart seed 0 each: bench.py checks its own results for them.
+SAMPLES = [
+    ("batched_1pct", sorted(random.Random(7).sample(range(4096), 41)), lambda i: synth.batched(30000 + i)),
+    ("stress_1pct", sorted(random.Random(8).sample(range(512), 5)), lambda i: synth.stress(40000 + i)),
+]
+
 
 def harness(path, seeds, passes, flags):
     assert seeds == list(range(seeds[0], seeds[0] + len(seeds))), "seeds must be contiguous"
@@ -157,6 +165,21 @@ def make_decoder() -> list:
                 rows.append({"case": name, "instance": ii, "inst_seed": inst.seed,
                              "sha256": hashlib.sha256(text.encode()).hexdigest(),
                              "seeds": seeds, "passes": passes, "flags": flags, "expected": got})
+        for name, idx, gen in SAMPLES:
+            for n, i in enumerate(idx):
+                inst = gen(i)
+                text = inst.to_thpack()
+                path = os.path.join(td, f"{name}_{i}.txt")
+                with open(path, "w") as f:
+                    f.write(text)
+                got = harness(path, [0], 1, [])
+                if n == 0:
+                    py = python_ref(text, 0, 1, [])
+                    if py != got[0]:
+                        raise SystemExit(f"g++ and CPython reference disagree on {name}/{i}")
+                rows.append({"case": name, "instance": n, "set_index": i, "inst_seed": inst.seed,
+                             "sha256": hashlib.sha256(text.encode()).hexdigest(),
+                             "seeds": [0], "passes": 1, "flags": [], "expected": got})
     return rows
 
 

@@ -140,3 +140,44 @@ def test_time_budget_on_device_equals_fixed_passes(inst_file):
     fixed = run([inst_file, "--passes", str(n), "--seed", "3", "--json"])
     assert fixed.returncode == 0
     assert _strip(fixed.stdout) == d
+
+
+def _multi_text(insts):
+    """One thpack file holding several instances (P = len(insts))."""
+    body = ["".join(i.to_thpack().splitlines(keepends=True)[1:]) for i in insts]
+    return f"{len(insts)}\n" + "".join(body)
+
+
+def test_multi_instance_file_needs_the_flag():
+    with tempfile.NamedTemporaryFile("w", suffix=".txt", delete=False) as f:
+        f.write(_multi_text([synth.single_pass(1), synth.batched(30001)]))
+    r = run([f.name, "--json"])
+    os.unlink(f.name)
+    assert r.returncode == 1
+    assert r.stderr.strip() == "instance error: expected exactly 1 instance, got 2"
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("extra", [["--single-pass"], ["--device", "4", "--single-pass"]])
+def test_multi_instance_file_in_one_launch(extra):
+    insts = [synth.single_pass(1), synth.batched(30001), synth.batched(30002)]
+    with tempfile.TemporaryDirectory() as d:
+        multi = os.path.join(d, "multi.txt")
+        open(multi, "w").write(_multi_text(insts))
+        r = run([multi, "--multi", "--json", "--seed", "2"] + extra)
+        assert r.returncode == 0, r.stderr
+        lines = r.stdout.strip().splitlines()
+        assert len(lines) == len(insts)
+        for i, inst in enumerate(insts):
+            one = os.path.join(d, f"one{i}.txt")
+            open(one, "w").write(inst.to_thpack())
+            single = run([one, "--json", "--seed", "2"] + extra)
+            assert single.returncode == 0
+            a, b = json.loads(lines[i]), json.loads(single.stdout)
+            if "rows" in a:
+                a, b = [_strip(json.dumps(x)) for x in a["rows"]], [_strip(json.dumps(x)) for x in b["rows"]]
+            else:
+                a, b = _strip(lines[i]), _strip(single.stdout)
+            assert a == b
+            if "--device" not in extra:
+                assert a == _ref([one, "--json", "--seed", "2", "--single-pass"])

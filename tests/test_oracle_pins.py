@@ -204,6 +204,12 @@ def _golden_cases():
 
 
 def _instance_for(case):
+    if "set_index" in case:   # 1 % samples of the bench's batched / stress sets
+        i = case["set_index"]
+        inst = synth.batched(30000 + i) if case["case"].startswith("batched") else synth.stress(40000 + i)
+        text = inst.to_thpack()
+        assert hashlib.sha256(text.encode()).hexdigest() == case["sha256"], "generator drifted"
+        return text
     gen = {"single_pass": lambda: [synth.single_pass(1)],
            "multi_restart": lambda: [synth.multi_restart(2)],
            "batched": lambda: synth.batched_set(8),
