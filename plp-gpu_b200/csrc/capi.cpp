@@ -134,6 +134,7 @@ struct Batch {
     const uint32_t* mt_init = nullptr;
     cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
     char* h_flag = nullptr;                // pinned error-flag word
+    bool own_ctx = true;                   // h_flag and ev allocated by this batch
     std::vector<int2> redo_host;
     int2* h_redo_stage(size_t n) { redo_host.resize(n); return redo_host.data(); }
     size_t scratch_bytes = 0;
@@ -262,7 +263,24 @@ struct Batch {
 struct Pinned {
     char* p = nullptr;
     size_t cap = 0;
-    ~Pinned() { if (p) cudaFreeHost(p); }
+    // error-flag word and timing events lent to this thread's one-shot
+    // batches (pinned allocation and event creation cost more than a solve's
+    // whole host side)
+    char* flag = nullptr;
+    cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+    ~Pinned() {
+        if (p) cudaFreeHost(p);
+        if (flag) cudaFreeHost(flag);
+        for (auto& e : ev)
+            if (e) cudaEventDestroy(e);
+    }
+    cudaError_t ensure_ctx() {
+        cudaError_t e = cudaSuccess;
+        if (!flag) e = cudaMallocHost(&flag, 64);
+        for (auto& v : ev)
+            if (e == cudaSuccess && !v) e = cudaEventCreate(&v);
+        return e;
+    }
     cudaError_t ensure(size_t n) {
         if (n <= cap) return cudaSuccess;
         if (p) cudaFreeHost(p);
@@ -307,15 +325,23 @@ int batch_release(Batch& b, cudaStream_t st) {
     if (b.d_mem) e = cudaFreeAsync(b.d_mem, st);
     b.d_mem = nullptr;
     cudaError_t e2 = cudaStreamSynchronize(st);
-    for (auto& ev : b.ev)
-        if (ev) { cudaEventDestroy(ev); ev = nullptr; }
-    if (b.h_flag) { cudaFreeHost(b.h_flag); b.h_flag = nullptr; }
+    if (b.own_ctx) {
+        for (auto& ev : b.ev)
+            if (ev) cudaEventDestroy(ev);
+        if (b.h_flag) cudaFreeHost(b.h_flag);
+    }
+    for (auto& ev : b.ev) ev = nullptr;
+    b.h_flag = nullptr;
     if (e != cudaSuccess) return set_cuda_error("batch free", e);
     if (e2 != cudaSuccess) return set_cuda_error("batch completion", e2);
     return PLP_OK;
 }
 
-int batch_prepare(Batch& b, cudaStream_t st, Pinned& pin, int sms, const TileConfig& tc) {
+// one_shot: the batch runs once and is released before this thread prepares
+// another, so it borrows the thread's flag word and events and its upload
+// needs no synchronisation of its own (the execution synchronises).
+int batch_prepare(Batch& b, cudaStream_t st, Pinned& pin, int sms, const TileConfig& tc,
+                  bool one_shot) {
     int status = PLP_OK;
     b.mt_init = device_mt_init(&status);
     if (!b.mt_init) return status;
@@ -328,12 +354,20 @@ int batch_prepare(Batch& b, cudaStream_t st, Pinned& pin, int sms, const TileCon
         return s;
     };
     cudaError_t e;
-    for (auto& ev : b.ev) {
-        e = cudaEventCreate(&ev);
-        if (e != cudaSuccess) return fail("event creation", e);
+    if (one_shot) {
+        e = pin.ensure_ctx();
+        if (e != cudaSuccess) return fail("pinned flag", e);
+        b.own_ctx = false;
+        b.h_flag = pin.flag;
+        for (int k = 0; k < 3; k++) b.ev[k] = pin.ev[k];
+    } else {
+        for (auto& ev : b.ev) {
+            e = cudaEventCreate(&ev);
+            if (e != cudaSuccess) return fail("event creation", e);
+        }
+        e = cudaMallocHost(&b.h_flag, 64);
+        if (e != cudaSuccess) return fail("pinned flag", e);
     }
-    e = cudaMallocHost(&b.h_flag, 64);
-    if (e != cudaSuccess) return fail("pinned flag", e);
     e = cudaMallocAsync(&b.d_mem, b.bytes, st);
     if (e != cudaSuccess) return fail("batch allocation", e);
     const size_t up = b.upload_bytes();
@@ -346,8 +380,10 @@ int batch_prepare(Batch& b, cudaStream_t st, Pinned& pin, int sms, const TileCon
     e = cudaMemcpyAsync(b.d_mem, pin.p, up, cudaMemcpyHostToDevice, st);
     if (e != cudaSuccess) return fail("batch upload", e);
     // the staging buffer is reused by the next batch of this thread
-    e = cudaStreamSynchronize(st);
-    if (e != cudaSuccess) return fail("batch upload", e);
+    if (!one_shot) {
+        e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return fail("batch upload", e);
+    }
     return PLP_OK;
 }
 
@@ -486,6 +522,9 @@ int batch_execute(Batch& b, cudaStream_t st, int sms, TileConfig& tile, ExecStat
     }
     const int2* d_work = reinterpret_cast<const int2*>(b.d_mem + b.o_work);
     int* d_flag = reinterpret_cast<int*>(b.d_mem + b.o_next + 8);
+    // decoder, error-flag copy and selection in one stream pass with a single
+    // synchronisation; a raised flag (rare) re-runs the affected restarts
+    // below and selects again
     cudaError_t e = cudaMemsetAsync(d_flag, 0, 8, st);
     if (e != cudaSuccess) return fail("flag reset", e);
     e = cudaEventRecord(b.ev[0], st);
@@ -494,6 +533,14 @@ int batch_execute(Batch& b, cudaStream_t st, int sms, TileConfig& tile, ExecStat
     if (e != cudaSuccess) return fail("decoder launch", e);
     x.launches++;
     e = cudaMemcpyAsync(b.h_flag, d_flag, 4, cudaMemcpyDeviceToHost, st);
+    if (e != cudaSuccess) return fail("flag copy", e);
+    {
+        int n = 0;
+        e = enqueue_select(b, st, &n);
+        x.launches += n;
+        if (e != cudaSuccess) return fail("select launch", e);
+    }
+    e = cudaEventRecord(b.ev[2], st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return fail("decoder", e);
     float ms = 0;
@@ -548,15 +595,15 @@ int batch_execute(Batch& b, cudaStream_t st, int sms, TileConfig& tile, ExecStat
         if (e != cudaSuccess) return fail("decoder relaunch", e);
         x.launches++;
     }
-    {
+    if (retried) {   // the first selection read unfinished restarts
         int n = 0;
         e = enqueue_select(b, st, &n);
         x.launches += n;
         if (e != cudaSuccess) return fail("select launch", e);
+        e = cudaEventRecord(b.ev[2], st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return fail("select", e);
     }
-    e = cudaEventRecord(b.ev[2], st);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    if (e != cudaSuccess) return fail("select", e);
     cudaEventElapsedTime(&ms, b.ev[0], b.ev[2]);
     x.device_ms = ms;
     if (graph && !retried) batch_capture(b, st, sms, t);
@@ -565,9 +612,34 @@ int batch_execute(Batch& b, cudaStream_t st, int sms, TileConfig& tile, ExecStat
     return PLP_OK;
 }
 
-int batch_fetch(Batch& b, cudaStream_t st) {
+// Results of at most 64 MB come through the thread's pinned staging buffer
+// (full-bandwidth copies); larger ones go straight to pageable memory.
+int batch_fetch(Batch& b, cudaStream_t st, Pinned* pin = nullptr) {
     b.heads.resize(b.n_slots);
     b.best.resize(b.desc.size());
+    const size_t hb = b.n_slots * sizeof(SlotHead), bb = b.desc.size() * sizeof(int2);
+    const size_t pb = b.best_only ? b.desc.size() * (size_t)b.max_stride * 8 : (size_t)b.n_places * 8;
+    if (pin && hb + bb + pb <= (64u << 20) && pin->ensure(hb + bb + pb + 64) == cudaSuccess) {
+        cudaError_t e = cudaMemcpyAsync(pin->p, b.d_mem + b.o_heads, hb, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(pin->p + hb, b.d_mem + b.o_best, bb, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess && pb)
+            e = cudaMemcpyAsync(pin->p + hb + bb, b.d_mem + (b.best_only ? b.o_gather : b.o_places), pb,
+                                cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) {
+            const int s = set_cuda_error("result copy", e);
+            std::string keep = plpb_last();
+            batch_release(b, st);
+            set_error(s, keep);
+            return s;
+        }
+        std::memcpy(b.heads.data(), pin->p, hb);
+        std::memcpy(b.best.data(), pin->p + hb, bb);
+        b.places.resize(std::max<size_t>(1, pb / 8));
+        std::memcpy(b.places.data(), pin->p + hb + bb, pb);
+        return PLP_OK;
+    }
     cudaError_t e = cudaMemcpyAsync(b.heads.data(), b.d_mem + b.o_heads, b.n_slots * sizeof(SlotHead),
                                     cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess)
@@ -604,11 +676,11 @@ size_t batch_d2h_bytes(const Batch& b) {
 
 // full synchronous run used by plp_solve and the serving workers
 int run_batch(Batch& b, cudaStream_t st, Pinned& pin, int sms, TileConfig& tile) {
-    int s = batch_prepare(b, st, pin, sms, tile);
+    int s = batch_prepare(b, st, pin, sms, tile, true);
     if (s != PLP_OK) return s;
     s = batch_execute(b, st, sms, tile, nullptr, false);
     if (s != PLP_OK) return s;
-    s = batch_fetch(b, st);
+    s = batch_fetch(b, st, &pin);
     if (s != PLP_OK) return s;
     return batch_release(b, st);
 }
@@ -1187,7 +1259,7 @@ int plp_autotune(plp_handle* h, const plp_instance* const* insts, int32_t n_inst
         if (s != PLP_OK) break;
         b.work = sample;
         TileConfig t = t0;
-        s = batch_prepare(b, h->sync_stream, h->sync_pin, h->sms, t);
+        s = batch_prepare(b, h->sync_stream, h->sync_pin, h->sms, t, true);
         if (s != PLP_OK) break;
         double ms = 1e30;
         for (int rep = 0; rep < 3 && s == PLP_OK; rep++) {
@@ -1422,7 +1494,7 @@ int plp_batch_prepare(plp_handle* h, const plp_instance* const* insts, int32_t n
         std::lock_guard<std::mutex> lk(h->mu);
         tile = h->tile;
     }
-    if (s == PLP_OK) s = batch_prepare(pb->b, h->sync_stream, h->sync_pin, h->sms, tile);
+    if (s == PLP_OK) s = batch_prepare(pb->b, h->sync_stream, h->sync_pin, h->sms, tile, false);
     if (s != PLP_OK) {
         record(h, s);
         return s;
