@@ -571,6 +571,330 @@ void orc_run(const orc_instance* inst, int64_t seed, int n_passes,
     free(cur); free(best_acc); free(best_all);
 }
 
+/* ------------------------------------------------------------------------ */
+/* Block-building engine: blockproof/plp_block.cpp:29-304                    */
+/* ------------------------------------------------------------------------ */
+
+/* one block shape: cnt = a*b*k copies of type ti in orientation oi as a
+ * bw x bd x bh stack (blockproof/plp_block.cpp:29-37) */
+typedef struct {
+    int ti, oi, a, b, k;
+    long long cnt;
+    int bw, bd, bh;
+} blk_shape;
+
+typedef struct {
+    blk_shape* cat;
+    int n_cat;
+    int** by_type;     /* per type: catalogue indices, shape precedence order */
+    int* n_by_type;
+    int (*ors)[6][3];
+    int* n_ors;
+} blk_tables;
+
+static const blk_shape* g_cmp_cat;   /* qsort context (single-threaded oracle) */
+
+/* most copies, tallest stack, widest base, then orientation index
+ * (blockproof/plp_block.cpp:41-47) */
+static int blk_prec_cmp(const void* pa, const void* pb) {
+    const blk_shape* x = &g_cmp_cat[*(const int*)pa];
+    const blk_shape* y = &g_cmp_cat[*(const int*)pb];
+    if (x->cnt != y->cnt) return x->cnt > y->cnt ? -1 : 1;
+    if (x->bh != y->bh) return x->bh > y->bh ? -1 : 1;
+    if (x->a != y->a) return x->a > y->a ? -1 : 1;
+    if (x->b != y->b) return x->b > y->b ? -1 : 1;
+    return x->oi < y->oi ? -1 : (x->oi > y->oi ? 1 : 0);
+}
+
+/* placement order: block volume desc, type, orientation, k, a, b
+ * (blockproof/plp_block.cpp:165-175) */
+static int blk_place_cmp(const void* pa, const void* pb) {
+    const blk_shape* s = &g_cmp_cat[*(const int*)pa];
+    const blk_shape* t = &g_cmp_cat[*(const int*)pb];
+    const long long vs = (long long)s->bw * s->bd * s->bh, vt = (long long)t->bw * t->bd * t->bh;
+    if (vs != vt) return vs > vt ? -1 : 1;
+    if (s->ti != t->ti) return s->ti < t->ti ? -1 : 1;
+    if (s->oi != t->oi) return s->oi < t->oi ? -1 : 1;
+    if (s->k != t->k) return s->k > t->k ? -1 : 1;
+    if (s->a != t->a) return s->a > t->a ? -1 : 1;
+    if (s->b != t->b) return s->b > t->b ? -1 : (s->b < t->b ? 1 : 0);
+    return 0;
+}
+
+static const orc_instance* g_cmp_inst;
+/* types: item volume desc, then index (blockproof/plp_block.cpp:135-139) */
+static int blk_type_cmp(const void* pa, const void* pb) {
+    const int x = *(const int*)pa, y = *(const int*)pb;
+    const orc_item* a = &g_cmp_inst->items[x];
+    const orc_item* b = &g_cmp_inst->items[y];
+    const long long vx = (long long)a->l * a->w * a->h, vy = (long long)b->l * b->w * b->h;
+    if (vx != vy) return vx > vy ? -1 : 1;
+    return x < y ? -1 : (x > y ? 1 : 0);
+}
+
+/* catalogue bounded by amax/bmax/kmax, the pallet and the quantity
+ * (blockproof/plp_block.cpp:237-256) */
+static void blk_build(const orc_instance* inst, const orc_block_cfg* cfg, blk_tables* T) {
+    const int nt = inst->n_types;
+    T->ors = malloc(sizeof(int[6][3]) * (size_t)(nt > 0 ? nt : 1));
+    T->n_ors = malloc(sizeof(int) * (size_t)(nt > 0 ? nt : 1));
+    int cap = 64;
+    T->cat = malloc(sizeof(blk_shape) * (size_t)cap);
+    T->n_cat = 0;
+    for (int ti = 0; ti < nt; ti++) {
+        T->n_ors[ti] = orc_orientations(&inst->items[ti], T->ors[ti]);
+        for (int oi = 0; oi < T->n_ors[ti]; oi++) {
+            const int w = T->ors[ti][oi][0], d = T->ors[ti][oi][1], h = T->ors[ti][oi][2];
+            for (int a = 1; a <= cfg->amax; a++) {
+                if (a * w > inst->L) break;
+                for (int b = 1; b <= cfg->bmax; b++) {
+                    if (b * d > inst->W) break;
+                    for (int k = 1; k <= cfg->kmax; k++) {
+                        if (k * h > inst->H) break;
+                        const long long cnt = (long long)a * b * k;
+                        if (cnt > inst->items[ti].qty) break;
+                        if (T->n_cat == cap) {
+                            cap *= 2;
+                            T->cat = realloc(T->cat, sizeof(blk_shape) * (size_t)cap);
+                        }
+                        blk_shape* s = &T->cat[T->n_cat++];
+                        s->ti = ti; s->oi = oi; s->a = a; s->b = b; s->k = k; s->cnt = cnt;
+                        s->bw = a * w; s->bd = b * d; s->bh = k * h;
+                    }
+                }
+            }
+        }
+    }
+    T->by_type = malloc(sizeof(int*) * (size_t)(nt > 0 ? nt : 1));
+    T->n_by_type = calloc((size_t)(nt > 0 ? nt : 1), sizeof(int));
+    for (int i = 0; i < T->n_cat; i++) T->n_by_type[T->cat[i].ti]++;
+    for (int ti = 0; ti < nt; ti++) {
+        T->by_type[ti] = malloc(sizeof(int) * (size_t)(T->n_by_type[ti] > 0 ? T->n_by_type[ti] : 1));
+        T->n_by_type[ti] = 0;
+    }
+    for (int i = 0; i < T->n_cat; i++) {
+        const int ti = T->cat[i].ti;
+        T->by_type[ti][T->n_by_type[ti]++] = i;
+    }
+    g_cmp_cat = T->cat;
+    for (int ti = 0; ti < nt; ti++)
+        if (T->n_by_type[ti] > 1)
+            qsort(T->by_type[ti], (size_t)T->n_by_type[ti], sizeof(int), blk_prec_cmp);
+}
+
+static void blk_free(const orc_instance* inst, blk_tables* T) {
+    for (int ti = 0; ti < inst->n_types; ti++) free(T->by_type[ti]);
+    free(T->by_type); free(T->n_by_type); free(T->cat); free(T->ors); free(T->n_ors);
+}
+
+/* bottom support and flush side contact of shape s at point p
+ * (blockproof/plp_block.cpp:68-84) */
+static void blk_contact(int x0, int y0, int z0, const blk_shape* s, const int32_t* fast, int n_fast,
+                        long long* bottom, long long* side) {
+    const long long x = x0, y = y0, z = z0, bw = s->bw, bd = s->bd, bh = s->bh;
+    long long bo = 0, si = 0;
+    if (z == 0) bo = bw * bd;
+    for (int j = 0; j < n_fast; j++) {
+        const int32_t* b = fast + 6 * j;
+        const long long ox = (x + bw < b[3] ? x + bw : b[3]) - (x > b[0] ? x : b[0]);
+        const long long oy = (y + bd < b[4] ? y + bd : b[4]) - (y > b[1] ? y : b[1]);
+        const long long oz = (z + bh < b[5] ? z + bh : b[5]) - (z > b[2] ? z : b[2]);
+        if (b[5] == z && ox > 0 && oy > 0) bo += ox * oy;
+        if (oy > 0 && oz > 0 && (b[3] == x || b[0] == x + bw)) si += oy * oz;
+        if (ox > 0 && oz > 0 && (b[4] == y || b[1] == y + bd)) si += ox * oz;
+    }
+    *bottom = bo;
+    *side = si;
+}
+
+static int blk_pass_t(const orc_instance* inst, const blk_tables* T, const orc_block_cfg* cfg,
+                      double eps, orc_rng* rng, orc_place* out) {
+    const int L = inst->L, W = inst->W, H = inst->H, nt = inst->n_types;
+    int total = 0;
+    for (int t = 0; t < nt; t++) total += inst->items[t].qty;
+    int* rem = malloc(sizeof(int) * (size_t)(nt > 0 ? nt : 1));
+    for (int t = 0; t < nt; t++) rem[t] = inst->items[t].qty;
+    int cap = 8 * total + 16;
+    int32_t* cand = malloc(sizeof(int32_t) * 3 * (size_t)cap);
+    int32_t* fast = malloc(sizeof(int32_t) * 6 * (size_t)(total > 0 ? total : 1));
+    int* bshape = malloc(sizeof(int) * (size_t)(total > 0 ? total : 1));   /* placed block shapes */
+    int* feas = malloc(sizeof(int) * (size_t)cap);
+    int* types = malloc(sizeof(int) * (size_t)(nt > 0 ? nt : 1));
+    int* plan = malloc(sizeof(int) * (size_t)(total > 0 ? total : 1));
+    int n_cand = 1, n_fast = 0;
+    cand[0] = cand[1] = cand[2] = 0;
+    for (;;) {
+        /* plan: every type with copies left, block decomposition per type */
+        int n_types = 0;
+        for (int ti = 0; ti < nt; ti++)
+            if (rem[ti] > 0 && T->n_ors[ti] > 0) types[n_types++] = ti;
+        if (n_types == 0) break;
+        g_cmp_inst = inst;
+        qsort(types, (size_t)n_types, sizeof(int), blk_type_cmp);
+        if (eps > 0.0 && orc_rng_random(rng) >= 1.0 - eps)
+            for (int i = n_types - 1; i > 0; i--) {
+                const int j = orc_rng_randrange(rng, i + 1);
+                const int tmp = types[i]; types[i] = types[j]; types[j] = tmp;
+            }
+        int n_plan = 0;
+        for (int q = 0; q < n_types; q++) {
+            const int ti = types[q];
+            int r = rem[ti];
+            const int* shp = T->by_type[ti];
+            const int ns = T->n_by_type[ti];
+            while (r > 0) {
+                int start = ns;
+                while (start > 0 && T->cat[shp[start - 1]].cnt <= r) start--;
+                if (start == ns) break;
+                const int tk = cfg->topk < ns - start ? cfg->topk : ns - start;
+                int pick = 0;
+                if (eps > 0.0 && orc_rng_random(rng) >= 1.0 - eps) pick = orc_rng_randrange(rng, tk);
+                plan[n_plan++] = shp[start + pick];
+                r -= (int)T->cat[shp[start + pick]].cnt;
+            }
+        }
+        if (n_plan == 0) break;
+        g_cmp_cat = T->cat;
+        qsort(plan, (size_t)n_plan, sizeof(int), blk_place_cmp);
+        /* placement: extreme-point insertion at block granularity */
+        int any = 0;
+        for (int q = 0; q < n_plan; q++) {
+            const blk_shape* s = &T->cat[plan[q]];
+            if (rem[s->ti] < s->cnt) continue;
+            int nf = 0;
+            for (int ci = 0; ci < n_cand; ci++)
+                if (orc_feasible_one(cand[3 * ci], cand[3 * ci + 1], cand[3 * ci + 2], s->bw, s->bd, s->bh,
+                                     fast, n_fast, L, W, H))
+                    feas[nf++] = ci;
+            if (nf == 0) continue;
+            int pc;
+            if (eps > 0.0 && orc_rng_random(rng) >= 1.0 - eps) {
+                pc = feas[orc_rng_randrange(rng, nf)];
+            } else if (cfg->pick == 0) {
+                pc = feas[0];
+            } else {
+                long long k0 = -1, k1 = -1;
+                int bi = 0;
+                for (int i = 0; i < nf; i++) {
+                    long long sup, side;
+                    blk_contact(cand[3 * feas[i]], cand[3 * feas[i] + 1], cand[3 * feas[i] + 2], s, fast,
+                                n_fast, &sup, &side);
+                    const long long p0 = cfg->pick == 1 ? sup : sup + side;
+                    const long long p1 = cfg->pick == 1 ? side : sup;
+                    if (p0 > k0 || (p0 == k0 && p1 > k1)) { k0 = p0; k1 = p1; bi = i; }
+                }
+                pc = feas[bi];
+            }
+            const int x = cand[3 * pc], y = cand[3 * pc + 1], z = cand[3 * pc + 2];
+            bshape[n_fast] = plan[q];
+            int32_t* f = fast + 6 * n_fast++;
+            f[0] = x; f[1] = y; f[2] = z; f[3] = x + s->bw; f[4] = y + s->bd; f[5] = z + s->bh;
+            /* extreme points: drop the strictly interior ones, add the 8 corners */
+            int m = 0;
+            for (int i = 0; i < n_cand; i++) {
+                const int px = cand[3 * i], py = cand[3 * i + 1], pz = cand[3 * i + 2];
+                if (x < px && px < x + s->bw && y < py && py < y + s->bd && z < pz && pz < z + s->bh) continue;
+                cand[3 * m] = px; cand[3 * m + 1] = py; cand[3 * m + 2] = pz;
+                m++;
+            }
+            for (int c = 0; c < 8; c++) {
+                cand[3 * m] = x + ((c & 1) ? s->bw : 0);
+                cand[3 * m + 1] = y + ((c & 2) ? s->bd : 0);
+                cand[3 * m + 2] = z + ((c & 4) ? s->bh : 0);
+                m++;
+            }
+            qsort(cand, (size_t)m, sizeof(int32_t) * 3, pt_cmp);
+            int u = 0;
+            for (int i = 0; i < m; i++) {
+                if (u > 0 && pt_cmp(cand + 3 * (u - 1), cand + 3 * i) == 0) continue;
+                if (u != i) memmove(cand + 3 * u, cand + 3 * i, sizeof(int32_t) * 3);
+                u++;
+            }
+            n_cand = u;
+            rem[s->ti] -= (int)s->cnt;
+            any = 1;
+        }
+        if (!any) break;
+    }
+    /* decompose the blocks into item boxes (blockproof/plp_block.cpp:210-222) */
+    int n = 0;
+    for (int j = 0; j < n_fast; j++) {
+        const blk_shape* s = &T->cat[bshape[j]];
+        const int iw = s->bw / s->a, id = s->bd / s->b, ih = s->bh / s->k;
+        for (int i = 0; i < s->a; i++)
+            for (int jj = 0; jj < s->b; jj++)
+                for (int t = 0; t < s->k; t++) {
+                    orc_place* o = &out[n++];
+                    o->type = s->ti;
+                    o->x = fast[6 * j] + i * iw; o->y = fast[6 * j + 1] + jj * id; o->z = fast[6 * j + 2] + t * ih;
+                    o->w = iw; o->d = id; o->h = ih;
+                }
+    }
+    free(rem); free(cand); free(fast); free(bshape); free(feas); free(types); free(plan);
+    return n;
+}
+
+int orc_block_pass(const orc_instance* inst, const orc_block_cfg* cfg, double eps, orc_rng* rng,
+                   orc_place* out) {
+    blk_tables T;
+    blk_build(inst, cfg, &T);
+    const int n = blk_pass_t(inst, &T, cfg, eps, rng, out);
+    blk_free(inst, &T);
+    return n;
+}
+
+/* run_block: blockproof/plp_block.cpp:228-304 (online best-of; the same
+ * outcome as run()'s stored packings) */
+void orc_block_run(const orc_instance* inst, int64_t seed, int n_passes, double time_limit_s,
+                   double eps, int has_theta, double theta, double mu, const orc_block_cfg* cfg,
+                   orc_result* res) {
+    orc_rng rng;
+    orc_rng_seed(&rng, (uint64_t)(seed < 0 ? -seed : seed));
+    blk_tables T;
+    blk_build(inst, cfg, &T);
+    int total = 0;
+    for (int t = 0; t < inst->n_types; t++) total += inst->items[t].qty;
+    const size_t cap = (size_t)(total > 0 ? total : 1);
+    orc_place* cur = malloc(sizeof(orc_place) * cap);
+    orc_place* best_acc = malloc(sizeof(orc_place) * cap);
+    orc_place* best_all = malloc(sizeof(orc_place) * cap);
+    int n_acc = -1, n_all = -1;
+    long long v_acc = -1, v_all = -1;
+    double s_acc = 0, s_all = 0;
+    const double t0 = now_s();
+    int k = 0;
+    for (;;) {
+        const int n = blk_pass_t(inst, &T, cfg, eps, &rng, cur);
+        k++;
+        long long vol = 0;
+        for (int i = 0; i < n; i++) vol += (long long)cur[i].w * cur[i].d * cur[i].h;
+        const double sc = orc_stability_score(cur, n, mu);
+        const int upd_all = vol > v_all || (vol == v_all && n > n_all);
+        const int upd_acc = (!has_theta || sc >= theta) && (n_acc < 0 || vol > v_acc || (vol == v_acc && n > n_acc));
+        if (upd_acc) {
+            n_acc = n; v_acc = vol; s_acc = sc;
+            memcpy(best_acc, cur, sizeof(orc_place) * (size_t)n);
+        }
+        if (upd_all) {
+            n_all = n; v_all = vol; s_all = sc;
+            memcpy(best_all, cur, sizeof(orc_place) * (size_t)n);
+        }
+        if (time_limit_s < 0 ? k >= n_passes : (now_s() - t0) >= time_limit_s) break;
+    }
+    const int use_acc = n_acc >= 0;
+    res->n_boxes = use_acc ? n_acc : n_all;
+    res->volume = use_acc ? v_acc : v_all;
+    res->score = use_acc ? s_acc : s_all;
+    res->fallback = !use_acc;
+    res->n_passes = k;
+    res->seed = seed;
+    res->placements = malloc(sizeof(orc_place) * (size_t)(res->n_boxes > 0 ? res->n_boxes : 1));
+    memcpy(res->placements, use_acc ? best_acc : best_all, sizeof(orc_place) * (size_t)res->n_boxes);
+    res->time_s = now_s() - t0;
+    free(cur); free(best_acc); free(best_all);
+    blk_free(inst, &T);
+}
+
 void orc_free_result(orc_result* r) {
     free(r->placements);
     r->placements = NULL;

@@ -119,6 +119,23 @@ void orc_run(const orc_instance* inst, int64_t seed, int n_passes,
              orc_stats* st);
 void orc_free_result(orc_result* r);
 
+/* ---- block-building engine (blockproof/plp_block.cpp) -------------------- */
+/* Block limits a x b x k, the top-k shape pick width and the pick rule among
+ * feasible points: 0 first, 1 support (bottom, then side contact), 2 contact
+ * (bottom + side, then bottom). */
+typedef struct {
+    int amax, bmax, kmax, topk, pick;
+} orc_block_cfg;
+
+/* One block pass; the placed blocks decomposed into item boxes (block order,
+ * then a, b, k loops). out must hold sum(qty) entries. Returns n items. */
+int orc_block_pass(const orc_instance* inst, const orc_block_cfg* cfg, double eps,
+                   orc_rng* rng, orc_place* out);
+/* run_block: passes with online best-of selection (theta, fallback). */
+void orc_block_run(const orc_instance* inst, int64_t seed, int n_passes, double time_limit_s,
+                   double eps, int has_theta, double theta, double mu,
+                   const orc_block_cfg* cfg, orc_result* res);
+
 /* ---- output ------------------------------------------------------------ */
 /* CPython float repr; buf >= 32 bytes. Returns strlen. */
 int orc_py_repr(double x, char* buf);

@@ -7,6 +7,10 @@
  *              [--passes N]    fixed pass count instead of a wall-clock budget
  *              [--restarts R]  one JSON line per restart, seeds seed..seed+R-1
  *              [--stats]       print work counters (pairs, AABB tests) as JSON
+ *              [--block [--amax A] [--bmax B] [--kmax K] [--topk N]
+ *                       [--pick first|support|contact]]
+ *                              the block-building engine (blockproof/plp_block.cpp
+ *                              flags and defaults: 3, 3, 4, 8, first; mu 0.2)
  *   plp_oracle --selftest      RNG + repr blocks (gpu/plp_gpu.cpp:43-66 layout)
  */
 #include "plp_oracle.h"
@@ -58,7 +62,8 @@ int main(int argc, char** argv) {
     long long seed = 0;
     double time_s = 300.0, eps = 0.3, theta = 0.9, mu = 0.2;
     int has_theta = 1, order = 0, first_fit = 0, single = 0, as_json = 0;
-    int passes = 0, restarts = 1, stats = 0;
+    int passes = 0, restarts = 1, stats = 0, block = 0;
+    orc_block_cfg bc = {3, 3, 4, 8, 0};
     const char* e = getenv("PLP_MU");
     if (e) mu = strtod(e, NULL);
     for (int i = 1; i < argc; i++) {
@@ -83,6 +88,18 @@ int main(int argc, char** argv) {
         else if (!strcmp(a, "--passes")) passes = atoi(NEXT());
         else if (!strcmp(a, "--restarts")) restarts = atoi(NEXT());
         else if (!strcmp(a, "--stats")) stats = 1;
+        else if (!strcmp(a, "--block")) block = 1;
+        else if (!strcmp(a, "--amax")) bc.amax = atoi(NEXT());
+        else if (!strcmp(a, "--bmax")) bc.bmax = atoi(NEXT());
+        else if (!strcmp(a, "--kmax")) bc.kmax = atoi(NEXT());
+        else if (!strcmp(a, "--topk")) bc.topk = atoi(NEXT());
+        else if (!strcmp(a, "--pick")) {
+            const char* v = NEXT();
+            if (!strcmp(v, "first")) bc.pick = 0;
+            else if (!strcmp(v, "support")) bc.pick = 1;
+            else if (!strcmp(v, "contact")) bc.pick = 2;
+            else { fprintf(stderr, "bad --pick: %s (first|support|contact)\n", v); return 2; }
+        }
         else if (a[0] != '-') path = a;
         else { fprintf(stderr, "unknown flag: %s\n", a); return 2; }
     }
@@ -106,8 +123,18 @@ int main(int argc, char** argv) {
         orc_result res;
         orc_stats st;
         memset(&st, 0, sizeof st);
-        orc_run(&insts[0], seed + r, fixed > 0 ? fixed : 1, fixed > 0 ? -1.0 : time_s, eps,
-                has_theta, theta, order, first_fit, mu, &res, stats ? &st : NULL);
+        if (block) {
+            orc_block_cfg c = bc;
+            if (c.amax < 1) c.amax = 1;
+            if (c.bmax < 1) c.bmax = 1;
+            if (c.kmax < 1) c.kmax = 1;
+            if (c.topk < 1) c.topk = 1;
+            orc_block_run(&insts[0], seed + r, fixed > 0 ? fixed : 1, fixed > 0 ? -1.0 : time_s, eps,
+                          has_theta, theta, mu, &c, &res);
+        } else {
+            orc_run(&insts[0], seed + r, fixed > 0 ? fixed : 1, fixed > 0 ? -1.0 : time_s, eps,
+                    has_theta, theta, order, first_fit, mu, &res, stats ? &st : NULL);
+        }
         if (stats) {
             printf("{\"seed\": %lld, \"steps\": %lld, \"pairs\": %lld, \"c2_pairs\": %lld, "
                    "\"aabb_full\": %lld, \"max_cand\": %lld, \"pairs_to_first\": %lld, "

@@ -11,6 +11,9 @@ Fixtures:
                      (>= 2**32) and negative seeds: random(), getrandbits(k),
                      randrange(n)
   repr_vectors.json  CPython repr() of doubles (random bit patterns, c/n ratios)
+  block.jsonl        the reference's block-building engine (blockproof/plp_block.cpp,
+                     built as oracle/_ref/plp_block) --single-pass --json on the
+                     synthetic instances under several configurations, time_s removed
   decoder.jsonl      per-restart JSON of the reference's g++ build
                      (gpu/plp_common.hpp via oracle/_ref/ref_harness) on the
                      seeded synthetic workloads, time_s removed; every case also
@@ -35,6 +38,37 @@ from plpb200 import synth  # noqa: E402
 
 REF = "/root/reference"
 HARNESS = os.path.join(REPO, "oracle", "_ref", "ref_harness")
+PLP_BLOCK = os.path.join(REPO, "oracle", "_ref", "plp_block")
+
+BLOCK_CONFIGS = [
+    ("default", []),
+    ("campaign", ["--amax", "4", "--bmax", "4", "--kmax", "6", "--eps", "0.5", "--theta", "0.9", "--topk", "64"]),
+    ("support", ["--pick", "support"]),
+    ("contact_greedy", ["--pick", "contact", "--eps", "0"]),
+    ("first_no_theta", ["--eps", "0", "--no-theta"]),
+]
+BLOCK_INSTANCES = [("single_pass", lambda: synth.single_pass(1)), ("multi_restart", lambda: synth.multi_restart(2)),
+                   ("batched_30001", lambda: synth.batched(30001)), ("stress_40000", lambda: synth.stress(40000))]
+
+
+def make_block() -> list:
+    rows = []
+    with tempfile.TemporaryDirectory() as td:
+        for iname, gen in BLOCK_INSTANCES:
+            inst = gen()
+            text = inst.to_thpack()
+            path = os.path.join(td, f"{iname}.txt")
+            with open(path, "w") as f:
+                f.write(text)
+            for cname, flags in BLOCK_CONFIGS:
+                for seed in (0, 1):
+                    out = subprocess.run([PLP_BLOCK, path, "--seed", str(seed), "--single-pass", "--json"] + flags,
+                                         capture_output=True, text=True, check=True).stdout
+                    d = json.loads(out)
+                    d.pop("time_s")
+                    rows.append({"instance": iname, "sha256": hashlib.sha256(text.encode()).hexdigest(),
+                                 "config": cname, "flags": flags, "seed": seed, "expected": d})
+    return rows
 
 
 def bits_of(x: float) -> str:
@@ -195,6 +229,11 @@ def main():
         for r in rows:
             f.write(json.dumps(r, separators=(",", ":")) + "\n")
     print("wrote", len(rows), "decoder cases")
+    brows = make_block()
+    with open(os.path.join(HERE, "block.jsonl"), "w") as f:
+        for r in brows:
+            f.write(json.dumps(r, separators=(",", ":")) + "\n")
+    print("wrote", len(brows), "block cases")
 
 
 if __name__ == "__main__":

@@ -41,6 +41,10 @@ class Stats(ctypes.Structure):
                                               "max_cand", "pairs_to_first", "random_steps")]
 
 
+class BlockCfg(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int) for n in ("amax", "bmax", "kmax", "topk", "pick")]
+
+
 class Res(ctypes.Structure):
     _fields_ = [("n_boxes", ctypes.c_int), ("volume", ctypes.c_int64), ("score", ctypes.c_double),
                 ("fallback", ctypes.c_int), ("n_passes", ctypes.c_int), ("time_s", ctypes.c_double),
@@ -80,6 +84,9 @@ def lib():
                               ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int,
                               ctypes.c_double, ctypes.POINTER(Res), ctypes.POINTER(Stats)]
         L.orc_free_result.argtypes = [ctypes.POINTER(Res)]
+        L.orc_block_run.argtypes = [ctypes.POINTER(Inst), ctypes.c_int64, ctypes.c_int, ctypes.c_double,
+                                    ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                    ctypes.POINTER(BlockCfg), ctypes.POINTER(Res)]
         L.orc_to_json.argtypes = [ctypes.POINTER(Res), ctypes.c_char_p, ctypes.c_int]
         L.orc_py_repr.argtypes = [ctypes.c_double, ctypes.c_char_p]
         L.orc_orientations.argtypes = [ctypes.POINTER(Item), ctypes.POINTER(ctypes.c_int * 3 * 6)]
@@ -216,3 +223,39 @@ def candidate_points(placed):
 
 def nan_or(theta):
     return math.nan if theta is None else theta
+
+
+PICKS = {"first": 0, "support": 1, "contact": 2}
+
+
+def run_block(inst: "OInstance", seed=0, passes=1, eps=0.3, theta=0.9, mu=0.2, amax=3, bmax=3, kmax=4,
+              topk=8, pick="first", i=0):
+    """Block-building engine (blockproof/plp_block.cpp), fixed pass count.
+    Returns the JSON line (time_s included)."""
+    r = Res()
+    cfg = BlockCfg(max(1, amax), max(1, bmax), max(1, kmax), max(1, topk), PICKS[pick])
+    has_theta = theta is not None
+    lib().orc_block_run(inst.at(i), int(seed), int(passes), -1.0, float(eps), 1 if has_theta else 0,
+                        float(theta) if has_theta else 0.0, float(mu), ctypes.byref(cfg), ctypes.byref(r))
+    need = lib().orc_to_json(ctypes.byref(r), None, 0)
+    buf = ctypes.create_string_buffer(need + 1)
+    lib().orc_to_json(ctypes.byref(r), buf, need + 1)
+    lib().orc_free_result(ctypes.byref(r))
+    return buf.value.decode()
+
+
+def block_flags_to_kw(flags):
+    """plp_block CLI flags -> run_block keyword arguments (reference defaults)."""
+    kw = dict(eps=0.3, theta=0.9, amax=3, bmax=3, kmax=4, topk=8, pick="first")
+    i = 0
+    while i < len(flags):
+        f = flags[i]
+        if f == "--no-theta":
+            kw["theta"] = None
+            i += 1
+            continue
+        v = flags[i + 1]
+        key = f[2:]
+        kw[key] = v if key == "pick" else (float(v) if key in ("eps", "theta") else int(v))
+        i += 2
+    return kw

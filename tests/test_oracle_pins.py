@@ -265,3 +265,25 @@ def test_oracle_matches_reference_cpython_eps():
             assert pl == [tuple(p) for p in r.placements]
             assert (s["n_boxes"], s["volume"], s["score"], s["fallback"]) == \
                 (r.n_boxes, r.volume, r.score, r.fallback)
+
+
+# ---------------------------------------------------------------- block engine
+def block_cases():
+    return [json.loads(l) for l in open(os.path.join(GOLDEN, "block.jsonl"))]
+
+
+def block_instance_text(case):
+    gen = {"single_pass": lambda: synth.single_pass(1), "multi_restart": lambda: synth.multi_restart(2),
+           "batched_30001": lambda: synth.batched(30001), "stress_40000": lambda: synth.stress(40000)}
+    text = gen[case["instance"]]().to_thpack()
+    assert hashlib.sha256(text.encode()).hexdigest() == case["sha256"], "generator drifted"
+    return text
+
+
+@pytest.mark.parametrize("case", block_cases(), ids=lambda c: f"{c['instance']}-{c['config']}-{c['seed']}")
+def test_oracle_block_matches_reference_block_engine(case):
+    """The C restatement of blockproof/plp_block.cpp against the reference's
+    own build (golden fixtures), --single-pass."""
+    js = O.run_block(O.OInstance(block_instance_text(case)), seed=case["seed"],
+                     **O.block_flags_to_kw(case["flags"]))
+    assert O.strip_time(js) == case["expected"]
