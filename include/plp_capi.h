@@ -118,6 +118,13 @@ typedef struct {
                              the summary's n_passes is the count run. */
     int32_t best_only;    /* 1: copy back the placements of the best restart only
                              (summaries of every restart are always returned) */
+    /* engine 1 is the block-building engine (blockproof/plp_block.cpp): items
+     * grouped into a x b x k blocks of one type and orientation, placed at
+     * extreme points; order and first_fit do not apply to it. */
+    int32_t engine;       /* 0 extreme-point decoder, 1 block-building engine */
+    int32_t blk_amax, blk_bmax, blk_kmax;   /* block limits (reference defaults 3, 3, 4) */
+    int32_t blk_topk;     /* eps pick among the top-k fitting shapes (default 8) */
+    int32_t blk_pick;     /* point rule: 0 first, 1 support, 2 contact */
 } plp_run_opts;
 
 void plp_default_opts(plp_run_opts* o);   /* reference CLI defaults */

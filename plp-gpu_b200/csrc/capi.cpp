@@ -104,16 +104,124 @@ void remember_tile(TileConfig& keep, const TileConfig& used) {
     if (!decoder_config_supported(keep.G, keep.D, keep.M)) keep.M = 1;
 }
 
-// Fewer decoders per CTA when the tile plus this batch's top-z index (Hz
-// entries) would not fit one CTA's shared memory.
-void fit_tile(TileConfig& t, int Hz) {
-    while (t.D > 1 && decoder_smem_bytes(t.P, t.C, Hz, t.G) * t.D > 227 * 1024) t.D >>= 1;
-    while (!decoder_config_supported(t.G, t.D, t.M) && t.D > 1) t.D >>= 1;
-    if (!decoder_config_supported(t.G, t.D, t.M)) t.M = 1;
-}
+
 
 constexpr int P_MAX = 2048;
 constexpr int C_MAX = 8192;
+
+struct Batch;
+// shared-memory bytes, supported launch shape and occupancy of a tile for a
+// batch's engine (extreme-point decoder or block engine)
+int tile_smem(const Batch& b, const TileConfig& t);
+bool tile_supported(const Batch& b, const TileConfig& t);
+cudaError_t tile_occupancy(const Batch& b, const TileConfig& t, int* occ);
+
+// Host tables of the block-building engine for one instance
+// (blockproof/plp_block.cpp:237-262): the shape catalogue; each type's shapes
+// in precedence order (most copies, tallest stack, widest base, orientation);
+// for each type the first shape fitting r remaining copies, for every r below
+// the type's largest count; the placement rank of every shape (block volume
+// desc, type, orientation, k desc, a desc, b desc) and the shapes by rank; the
+// type order (volume desc, index) and the copies per type.
+int build_block_tables(const Instance& I, const std::vector<TypeOrs>& ors, const plp_run_opts& o,
+                       std::vector<BlkShape>& cat_all, std::vector<int>& tab, InstDesc& d) {
+    const int amax = std::max(1, o.blk_amax), bmax = std::max(1, o.blk_bmax), kmax = std::max(1, o.blk_kmax);
+    const int nt = (int)I.types.size();
+    std::vector<BlkShape> cat;
+    for (int ti = 0; ti < nt; ti++) {
+        for (int oi = 0; oi < ors[ti].n; oi++) {
+            const int w = ors[ti].w[oi], dd = ors[ti].d[oi], h = ors[ti].h[oi];
+            for (int a = 1; a <= amax; a++) {
+                if ((long long)a * w > I.L) break;
+                for (int b = 1; b <= bmax; b++) {
+                    if ((long long)b * dd > I.W) break;
+                    for (int k = 1; k <= kmax; k++) {
+                        if ((long long)k * h > I.H) break;
+                        const long long cnt = 1LL * a * b * k;
+                        if (cnt > I.types[ti].qty) break;
+                        if (cat.size() >= (size_t)(1 << 22))
+                            return set_error(PLP_E_CAPACITY, "block catalogue larger than 4M shapes");
+                        cat.push_back(BlkShape{ti, oi, a, b, k, (int)cnt, a * w, b * dd, k * h, 0});
+                    }
+                }
+            }
+        }
+    }
+    const int nc = (int)cat.size();
+    std::vector<std::vector<int>> by(nt);
+    for (int i = 0; i < nc; i++) by[cat[i].ti].push_back(i);
+    for (auto& v : by)
+        std::sort(v.begin(), v.end(), [&](int x, int y) {
+            const BlkShape &p = cat[x], &q = cat[y];
+            if (p.cnt != q.cnt) return p.cnt > q.cnt;
+            if (p.bh != q.bh) return p.bh > q.bh;
+            if (p.a != q.a) return p.a > q.a;
+            if (p.b != q.b) return p.b > q.b;
+            return p.oi < q.oi;
+        });
+    std::vector<int> by_rank(nc);
+    for (int i = 0; i < nc; i++) by_rank[i] = i;
+    std::sort(by_rank.begin(), by_rank.end(), [&](int x, int y) {
+        const BlkShape &p = cat[x], &q = cat[y];
+        const long long vp = 1LL * p.bw * p.bd * p.bh, vq = 1LL * q.bw * q.bd * q.bh;
+        if (vp != vq) return vp > vq;
+        if (p.ti != q.ti) return p.ti < q.ti;
+        if (p.oi != q.oi) return p.oi < q.oi;
+        if (p.k != q.k) return p.k > q.k;
+        if (p.a != q.a) return p.a > q.a;
+        return p.b > q.b;
+    });
+    for (int r = 0; r < nc; r++) cat[by_rank[r]].rank = r;
+    std::vector<int> tord(nt);
+    for (int t = 0; t < nt; t++) tord[t] = t;
+    std::sort(tord.begin(), tord.end(), [&](int x, int y) {
+        const long long vx = I.types[x].volume(), vy = I.types[y].volume();
+        if (vx != vy) return vx > vy;
+        return x < y;
+    });
+    d.n_types = nt;
+    d.bo_order = (int)tab.size();
+    tab.insert(tab.end(), tord.begin(), tord.end());
+    d.bo_qty = (int)tab.size();
+    for (int t = 0; t < nt; t++) tab.push_back(I.types[t].qty);
+    d.bo_list_off = (int)tab.size();
+    {
+        int off = 0;
+        for (int t = 0; t < nt; t++) { tab.push_back(off); off += (int)by[t].size(); }
+        tab.push_back(off);
+    }
+    d.bo_list = (int)tab.size();
+    for (int t = 0; t < nt; t++) tab.insert(tab.end(), by[t].begin(), by[t].end());
+    d.bo_start_off = (int)tab.size();
+    {
+        int off = 0;
+        for (int t = 0; t < nt; t++) {
+            tab.push_back(off);
+            off += by[t].empty() ? 0 : cat[by[t][0]].cnt - 1;
+        }
+        tab.push_back(off);
+    }
+    d.bo_start = (int)tab.size();
+    for (int t = 0; t < nt; t++) {
+        if (by[t].empty()) continue;
+        const int maxc = cat[by[t][0]].cnt, ns = (int)by[t].size();
+        for (int r = 1; r < maxc; r++) {   // shapes are cnt-desc: the fitting ones form a suffix
+            int start = ns;
+            while (start > 0 && cat[by[t][start - 1]].cnt <= r) start--;
+            tab.push_back(start);
+        }
+    }
+    d.bo_shape_of_rank = (int)tab.size();
+    tab.insert(tab.end(), by_rank.begin(), by_rank.end());
+    d.cat_off = (int)cat_all.size();
+    d.n_cat = nc;
+    cat_all.insert(cat_all.end(), cat.begin(), cat.end());
+    d.blk_topk = std::max(1, o.blk_topk);
+    d.blk_pick = o.blk_pick;
+    if (tab.size() > (size_t)INT_MAX / 2 || cat_all.size() > (size_t)INT_MAX / 2)
+        return set_error(PLP_E_CAPACITY, "block tables too large for one batch");
+    return PLP_OK;
+}
 
 struct Batch {
     std::vector<const Instance*> insts;
@@ -127,10 +235,14 @@ struct Batch {
     long long n_slots = 0, n_places = 0;
     int max_stride = 1, max_steps = 0, Hz = 0;
     bool multi_pass = false;
+    // block-building engine: shape catalogue and per-instance orderings
+    int engine = 0, max_types = 0;
+    std::vector<BlkShape> bcat;
+    std::vector<int> btab;
     // device
     char* d_mem = nullptr;
     size_t bytes = 0;
-    size_t o_desc, o_steps, o_types, o_work, o_next, o_heads, o_places, o_best, o_scratch, o_gather, o_redo;
+    size_t o_desc, o_steps, o_types, o_bcat, o_btab, o_work, o_next, o_heads, o_places, o_best, o_scratch, o_gather, o_redo;
     const uint32_t* mt_init = nullptr;
     cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
     char* h_flag = nullptr;                // pinned error-flag word
@@ -157,6 +269,9 @@ struct Batch {
         insts = in;
         opts = op;
         desc.clear(); steps.clear(); types.clear(); work.clear(); inst_ors.clear();
+        bcat.clear(); btab.clear();
+        engine = op.empty() ? 0 : op[0].engine;
+        max_types = 0;
         n_slots = 0; n_places = 0; max_stride = 1; max_steps = 0; multi_pass = false;
         int maxH = 0;
         best_only = true;
@@ -167,6 +282,13 @@ struct Batch {
             if (o.restarts < 1 || o.passes < 0 || (!budget && o.passes < 1))
                 return set_error(PLP_E_INVALID, "restarts must be >= 1 and passes >= 1 (>= 0 with a time limit)");
             if (o.order != 0 && o.order != 1) return set_error(PLP_E_INVALID, "order must be 0 or 1");
+            if (o.engine != 0 && o.engine != 1) return set_error(PLP_E_INVALID, "engine must be 0 or 1");
+            if (o.engine != engine)
+                return set_error(PLP_E_INVALID, "all instances of one batch must use the same engine");
+            if (o.engine == 1 && (o.blk_pick < 0 || o.blk_pick > 2))
+                return set_error(PLP_E_INVALID, "blk_pick must be 0 (first), 1 (support) or 2 (contact)");
+            if (o.engine == 1 && I.types.size() > 2048)
+                return set_error(PLP_E_CAPACITY, "the block engine takes at most 2048 box types");
             int xb = 0, yb = 0, zb = 0;
             for (int v = I.L; v; v >>= 1) xb++;
             for (int v = I.W; v; v >>= 1) yb++;
@@ -207,6 +329,13 @@ struct Batch {
                 ot.push_back(to);
                 types.push_back(to);
             }
+            desc.back().engine = o.engine;
+            desc.back().n_types = (int)I.types.size();
+            max_types = std::max(max_types, (int)I.types.size());
+            if (o.engine == 1) {
+                const int sb = build_block_tables(I, ot, o, bcat, btab, desc.back());
+                if (sb != PLP_OK) return sb;
+            }
             inst_ors.push_back(std::move(ot));
             n_slots += o.restarts;
             n_places += (long long)o.restarts * d.place_stride;
@@ -237,7 +366,7 @@ struct Batch {
     void plan(int sms, const TileConfig& t) {
         tile = t;
         int occ = 1;
-        if (decoder_occupancy(t.P, t.C, Hz, t.G, t.D, t.M, &occ) != cudaSuccess || occ < 1) occ = 1;
+        if (tile_occupancy(*this, t, &occ) != cudaSuccess || occ < 1) occ = 1;
         const long long need = (n_slots + t.D - 1) / t.D;
         ctas = (int)std::max(1LL, std::min<long long>(need, (long long)sms * occ));
         scratch_bytes = multi_pass ? (size_t)ctas * t.D * max_stride * 8 : 0;
@@ -245,6 +374,8 @@ struct Batch {
         o_desc = o;    o = al(o + desc.size() * sizeof(InstDesc));
         o_steps = o;   o = al(o + std::max<size_t>(1, steps.size()) * sizeof(int));
         o_types = o;   o = al(o + std::max<size_t>(1, types.size()) * sizeof(TypeOrs));
+        o_bcat = o;    o = al(o + std::max<size_t>(1, bcat.size()) * sizeof(BlkShape));
+        o_btab = o;    o = al(o + std::max<size_t>(1, btab.size()) * sizeof(int));
         o_work = o;    o = al(o + work.size() * sizeof(int2));
         o_next = o;    o = al(o + 16);
         o_heads = o;   o = al(o + n_slots * sizeof(SlotHead));
@@ -258,6 +389,31 @@ struct Batch {
 
     size_t upload_bytes() const { return o_next; }   // desc .. work are contiguous at the front
 };
+
+int tile_smem(const Batch& b, const TileConfig& t) {
+    return b.engine == 1 ? block_smem_bytes(t.P, t.C, std::max(1, b.max_steps), std::max(1, b.max_types), b.Hz)
+                         : decoder_smem_bytes(t.P, t.C, b.Hz, t.G);
+}
+
+bool tile_supported(const Batch& b, const TileConfig& t) {
+    return b.engine == 1 ? t.G == 1 && block_config_supported(t.D, t.M) : decoder_config_supported(t.G, t.D, t.M);
+}
+
+cudaError_t tile_occupancy(const Batch& b, const TileConfig& t, int* occ) {
+    if (b.engine == 1)
+        return block_occupancy(t.P, t.C, std::max(1, b.max_steps), std::max(1, b.max_types), b.Hz, t.D, t.M, occ);
+    return decoder_occupancy(t.P, t.C, b.Hz, t.G, t.D, t.M, occ);
+}
+
+// Fewer decoders per CTA when the tile plus this batch's top-z index (and,
+// for the block engine, its item and type tables) would not fit one CTA's
+// shared memory. The block engine runs one warp per restart.
+void fit_tile(TileConfig& t, const Batch& b) {
+    if (b.engine == 1) t.G = 1;
+    while (t.D > 1 && tile_smem(b, t) * t.D > 227 * 1024) t.D >>= 1;
+    while (!tile_supported(b, t) && t.D > 1) t.D >>= 1;
+    if (!tile_supported(b, t)) t.M = 1;
+}
 
 // pinned staging buffer per thread (grows)
 struct Pinned {
@@ -376,6 +532,8 @@ int batch_prepare(Batch& b, cudaStream_t st, Pinned& pin, int sms, const TileCon
     std::memcpy(pin.p + b.o_desc, b.desc.data(), b.desc.size() * sizeof(InstDesc));
     std::memcpy(pin.p + b.o_steps, b.steps.data(), b.steps.size() * sizeof(int));
     std::memcpy(pin.p + b.o_types, b.types.data(), b.types.size() * sizeof(TypeOrs));
+    if (!b.bcat.empty()) std::memcpy(pin.p + b.o_bcat, b.bcat.data(), b.bcat.size() * sizeof(BlkShape));
+    if (!b.btab.empty()) std::memcpy(pin.p + b.o_btab, b.btab.data(), b.btab.size() * sizeof(int));
     std::memcpy(pin.p + b.o_work, b.work.data(), b.work.size() * sizeof(int2));
     e = cudaMemcpyAsync(b.d_mem, pin.p, up, cudaMemcpyHostToDevice, st);
     if (e != cudaSuccess) return fail("batch upload", e);
@@ -404,11 +562,16 @@ static DecodeLaunch make_launch(const Batch& b, const TileConfig& t, const int2*
     L.P = t.P;
     L.C = t.C;
     L.Hz = b.Hz;
+    L.engine = b.engine;
+    L.bcat = reinterpret_cast<const BlkShape*>(b.d_mem + b.o_bcat);
+    L.btab = reinterpret_cast<const int*>(b.d_mem + b.o_btab);
+    L.N = std::max(1, b.max_steps);
+    L.T = std::max(1, b.max_types);
     L.warps_per_decoder = t.G;
     L.decoders_per_cta = t.D;
     L.min_blocks = t.M;
     int occ = 1;
-    if (decoder_occupancy(t.P, t.C, b.Hz, t.G, t.D, t.M, &occ) != cudaSuccess || occ < 1) occ = 1;
+    if (tile_occupancy(b, t, &occ) != cudaSuccess || occ < 1) occ = 1;
     L.ctas = (int)std::max<long long>(1, std::min<long long>((n_work + t.D - 1) / t.D, (long long)sms * occ));
     // multi-pass scratch holds one placement row per resident decoder
     if (b.multi_pass) {
@@ -496,7 +659,7 @@ int batch_execute(Batch& b, cudaStream_t st, int sms, TileConfig& tile, ExecStat
     };
     ExecStats x;
     TileConfig t = tile;
-    fit_tile(t, b.Hz);
+    fit_tile(t, b);
     if (b.gexec && same_tile(t, b.gtile)) {
         // replay: one graph launch, one synchronisation
         cudaError_t e = cudaEventRecord(b.ev[0], st);
@@ -578,10 +741,9 @@ int batch_execute(Batch& b, cudaStream_t st, int sms, TileConfig& tile, ExecStat
         if (grow_p) t.P = std::min(P_MAX, std::max(t.P * 2, 32));
         if (grow_c) t.C = std::min(C_MAX, t.C * 2);
         // deeper tiles: fewer decoders per CTA keeps one CTA within 227 KB
-        while (t.D > 1 && decoder_smem_bytes(t.P, t.C, b.Hz, t.G) * t.D > 200 * 1024) t.D >>= 1;
-        while (!decoder_config_supported(t.G, t.D, t.M) && t.D > 1) t.D >>= 1;
-        if (!decoder_config_supported(t.G, t.D, t.M)) t.M = 1;
-        if (decoder_smem_bytes(t.P, t.C, b.Hz, t.G) > 227 * 1024 || !decoder_config_supported(t.G, t.D, t.M)) {
+        while (t.D > 1 && tile_smem(b, t) * t.D > 200 * 1024) t.D >>= 1;
+        fit_tile(t, b);
+        if (tile_smem(b, t) > 227 * 1024 || !tile_supported(b, t)) {
             batch_release(b, st);
             return set_error(PLP_E_CAPACITY, "instance needs a larger tile than shared memory holds");
         }
@@ -897,6 +1059,12 @@ void plp_default_opts(plp_run_opts* o) {
     o->mu = 0.2;
     o->time_limit_s = -1.0;
     o->best_only = 0;
+    o->engine = 0;
+    o->blk_amax = 3;
+    o->blk_bmax = 3;
+    o->blk_kmax = 4;
+    o->blk_topk = 8;
+    o->blk_pick = 0;
 }
 
 // ---- instances -----------------------------------------------------------
@@ -1241,8 +1409,8 @@ int plp_autotune(plp_handle* h, const plp_instance* const* insts, int32_t n_inst
             for (const auto& x : dm) {
                 TileConfig t;
                 t.P = p; t.C = c; t.G = 1; t.D = x[0]; t.M = x[1];
-                fit_tile(t, full.Hz);
-                if (decoder_smem_bytes(t.P, t.C, full.Hz, t.G) * t.D > 227 * 1024) continue;
+                fit_tile(t, full);
+                if (tile_smem(full, t) * t.D > 227 * 1024) continue;
                 bool dup = false;
                 for (const auto& u : cand) dup = dup || same_tile(u, t);
                 if (!dup) cand.push_back(t);
@@ -1572,6 +1740,8 @@ int plp_decode_noalloc(const plp_instance* inst, const plp_run_opts* opts, void*
         return set_error(PLP_E_INVALID, "plp_decode_noalloc: null argument");
     if (opts->restarts < 1 || opts->passes < 1 || (opts->order != 0 && opts->order != 1))
         return set_error(PLP_E_INVALID, "plp_decode_noalloc: bad options");
+    if (opts->engine != 0)
+        return set_error(PLP_E_INVALID, "plp_decode_noalloc: extreme-point decoder only (engine 0)");
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     Batch b;
     int s = b.build({&inst->inst}, {*opts});

@@ -31,6 +31,27 @@ struct InstDesc {
     int has_theta, first_fit;
     long long budget_ns; // >= 0: passes (at most `passes`) until this much
                          // global-timer time has passed since the restart began
+    // block-building engine (engine == 1): offsets of this instance's tables
+    // in the launch's block table (ints) and shape catalogue
+    int engine;          // 0 extreme-point decoder, 1 block-building engine
+    int n_types;
+    int blk_topk, blk_pick;
+    int bo_order;        // types by (volume desc, index)
+    int bo_qty;          // copies per type
+    int bo_list;         // per type: catalogue indices in shape precedence order
+    int bo_list_off;     // n_types + 1 offsets into that list
+    int bo_start;        // per type: first fitting list index for r < max count
+    int bo_start_off;    // n_types + 1 offsets into that table
+    int bo_shape_of_rank;
+    int cat_off, n_cat;
+};
+
+// Block shape of the block-building engine (blockproof/plp_block.cpp:29-37):
+// cnt = a*b*k copies of type ti in orientation oi as a bw x bd x bh stack;
+// rank = its position in the placement order (block volume desc, type,
+// orientation, k desc, a desc, b desc; blockproof/plp_block.cpp:165-175).
+struct BlkShape {
+    int ti, oi, a, b, k, cnt, bw, bd, bh, rank;
 };
 
 // Nanoseconds of the GPU's global timer (one clock for all SMs).

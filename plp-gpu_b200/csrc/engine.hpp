@@ -22,6 +22,10 @@ struct DecodeLaunch {
     const uint32_t* mt_init;
     int P, C;                 // shared-memory tile: boxes and live points per decoder
     int Hz;                   // entries of the top-z index (max height + 2), 0 = none
+    int engine;               // 0 extreme-point decoder, 1 block-building engine
+    const BlkShape* bcat;     // block engine: shape catalogue of the batch
+    const int* btab;          // block engine: per-instance orderings (ints)
+    int N, T;                 // block engine tile: items, types per decoder
     int warps_per_decoder;    // G
     int decoders_per_cta;     // D
     int min_blocks;           // M (register cap through the launch bounds)
@@ -34,6 +38,12 @@ cudaError_t decoder_occupancy(int P, int C, int Hz, int G, int D, int M, int* ct
 cudaError_t launch_decoder(const DecodeLaunch& L, cudaStream_t st);     // configure + enqueue
 cudaError_t configure_decoder(const DecodeLaunch& L);                    // function attributes
 cudaError_t enqueue_decoder(const DecodeLaunch& L, cudaStream_t st);     // stream operations only
+// block-building engine (block.cu); one warp per restart, D decoders per CTA
+int block_smem_bytes(int P, int C, int N, int T, int Hz);
+bool block_config_supported(int D, int M);
+cudaError_t block_occupancy(int P, int C, int N, int T, int Hz, int D, int M, int* ctas_per_sm);
+cudaError_t configure_block(const DecodeLaunch& L);
+cudaError_t enqueue_block(const DecodeLaunch& L, cudaStream_t st);
 cudaError_t launch_select_best(const InstDesc* inst, int n_inst, const SlotHead* heads, int2* best,
                                cudaStream_t st);
 cudaError_t launch_rng_dump(const long long* seeds, int n_seeds, int n_random, int n_bits,

@@ -38,6 +38,12 @@ __device__ __forceinline__ int lower_bound_top(const int* z2, int n, int z) {
     return lo;
 }
 
+// First box with top >= z from the top-z index zt (zt[z] = boxes with top
+// < z), or by binary search when there is no index.
+__device__ __forceinline__ int box_start(const unsigned short* zt, const int* z2, int nb, int z) {
+    return zt ? (int)zt[z] : lower_bound_top(z2, nb, z);
+}
+
 // Bit o of the result: orientation o (w = ow[o], d = od[o], h = oh[o]) at
 // point (x, y, z) is feasible. Acc is the support-area accumulator type
 // (int when the container area is known to fit, long long otherwise).

@@ -48,6 +48,12 @@ class RunOpts(ctypes.Structure):
         ("mu", ctypes.c_double),
         ("time_limit_s", ctypes.c_double),
         ("best_only", ctypes.c_int32),
+        ("engine", ctypes.c_int32),
+        ("blk_amax", ctypes.c_int32),
+        ("blk_bmax", ctypes.c_int32),
+        ("blk_kmax", ctypes.c_int32),
+        ("blk_topk", ctypes.c_int32),
+        ("blk_pick", ctypes.c_int32),
     ]
 
 
@@ -149,7 +155,8 @@ def _ptr(a: np.ndarray):
 
 
 def make_opts(seed=0, restarts=1, passes=1, eps=0.3, theta=0.9, order="volume", first_fit=False,
-              mu=0.2, time_limit_s=-1.0, best_only=False) -> RunOpts:
+              mu=0.2, time_limit_s=-1.0, best_only=False, engine="ep", amax=3, bmax=3, kmax=4, topk=8,
+              pick="first") -> RunOpts:
     o = RunOpts()
     o.seed = int(seed)
     o.restarts = int(restarts)
@@ -161,6 +168,9 @@ def make_opts(seed=0, restarts=1, passes=1, eps=0.3, theta=0.9, order="volume", 
     o.mu = float(mu)
     o.time_limit_s = float(time_limit_s)
     o.best_only = 1 if best_only else 0
+    o.engine = {"ep": 0, "block": 1}[engine] if isinstance(engine, str) else int(engine)
+    o.blk_amax, o.blk_bmax, o.blk_kmax, o.blk_topk = int(amax), int(bmax), int(kmax), int(topk)
+    o.blk_pick = {"first": 0, "support": 1, "contact": 2}[pick] if isinstance(pick, str) else int(pick)
     return o
 
 
