@@ -61,6 +61,11 @@ def workload(name: str, rank: int):
         insts = synth.stress_set(512)
         R = 4096
         desc = "stress: 512 instances x 100 types, 4096 restarts each, eps 0.3, theta 0.9, 1 pass"
+    elif name == "block":
+        insts = synth.batched_set(512)
+        R = 64
+        desc = ("block: block-building engine, 512 batched instances, 64 restarts each, amax 4 bmax 4 "
+                "kmax 6 eps 0.5 topk 64 pick first, theta 0.9, 1 pass")
     elif name == "single_pass":
         insts = [synth.single_pass(1)]
         R = 1
@@ -68,6 +73,8 @@ def workload(name: str, rank: int):
     else:
         raise SystemExit(f"unknown workload {name}")
     kw = dict(eps=0.0, theta=None) if name == "single_pass" else dict(eps=0.3, theta=0.9)
+    if name == "block":
+        kw = dict(eps=0.5, theta=0.9, engine="block", amax=4, bmax=4, kmax=6, topk=64)
     seed = (1 if name == "single_pass" else 0) + rank * R
     opts = P.make_opts(seed=seed, restarts=R, **kw)
     return insts, opts, desc, R
@@ -269,7 +276,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="multi_restart",
-                    choices=["multi_restart", "batched", "stress", "single_pass"])
+                    choices=["multi_restart", "batched", "stress", "single_pass", "block"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
@@ -328,7 +335,8 @@ def main():
     # the results of an evenly spaced sample of at most 512 restarts
     slots = [(r, k) for r in warm_results for k in range(r.restarts)]
     stride = max(1, len(slots) // 512)
-    T = [r.work(k)[0] for r, k in slots[::stride]]
+    # (the block engine has no reference work replay: its roofline reports time only)
+    T = [r.work(k)[0] for r, k in slots[::stride]] if args.workload != "block" else [0]
     t_mean = sum(T) / len(T)
     clocks = Clocks(local)
     barrier()
@@ -371,9 +379,12 @@ def main():
         achieved = t_mean * R * len(insts) * INT_OPS_PER_AABB / (dec_mean_ms / 1000.0) / 1e12
         prof = read_profile_inputs()
         traffic = prof.get(f"traffic_bytes_per_launch.{args.workload}")
+        if args.workload == "block":   # no reference work replay for the block engine
+            achieved = None
         roofline = {
             "bound": "int32", "achieved": achieved, "peak": int_peak, "unit": "Tint-op/s",
-            "frac": achieved / int_peak, "traffic": float(traffic) if traffic else None,
+            "frac": achieved / int_peak if achieved is not None else None,
+            "traffic": float(traffic) if traffic else None,
             "peak_source": f"{props.multi_processor_count} SMs x 128 INT32 lanes x {sm_max:.0f} MHz "
                            "(sm_max_mhz of MEASURED_PEAKS.json)",
             "work_unit": f"reference AABB tests per decode T = {t_mean:.0f} (mean over {len(T)} of the "
@@ -384,7 +395,8 @@ def main():
             if f"fp64_pipe_pct.{args.workload}" in prof else None,
             "note": "T counts the reference's full C1/C3 scans; the incremental decoder skips most of "
                     "them, so frac can exceed 1. issue_active_pct_ncu is the hardware's own measure.",
-            "kernel": "decoder1_kernel" if tile[2] == 1 else "decoder_kernel",
+            "kernel": ("block_kernel" if args.workload == "block"
+                       else "decoder1_kernel" if tile[2] == 1 else "decoder_kernel"),
             "kernel_ms_per_launch": dec_mean_ms,
         }
         cpu = None

@@ -19,6 +19,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 PKG_DIR = os.path.dirname(_HERE)
 LIB_PATH = os.path.join(PKG_DIR, "libplp_b200.so")
 CLI_PATH = os.path.join(PKG_DIR, "plp_gpu")
+BLOCK_CLI_PATH = os.path.join(os.path.dirname(CLI_PATH), "plp_block")
 HEADER_PATH = os.path.join(os.path.dirname(PKG_DIR), "include", "plp_capi.h")
 
 OK, E_INVALID, E_FORMAT, E_CUDA, E_CAPACITY, E_BUDGET, E_TIMEOUT, E_NOT_FOUND, E_CANCELLED, \
