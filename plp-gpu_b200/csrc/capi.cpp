@@ -261,6 +261,9 @@ struct Batch {
     std::vector<SlotHead> heads;
     std::vector<int2> best;
     std::vector<unsigned long long> places;   // all slots, or gathered best per instance
+    // where the fetched placements are: places.data(), or the fetching
+    // thread's pinned staging buffer (valid until that thread's next batch)
+    const unsigned long long* places_ptr = nullptr;
     bool best_only = false;
     double t_start = 0, t_end = 0;
 
@@ -774,14 +777,17 @@ int batch_execute(Batch& b, cudaStream_t st, int sms, TileConfig& tile, ExecStat
     return PLP_OK;
 }
 
-// Results of at most 64 MB come through the thread's pinned staging buffer
-// (full-bandwidth copies); larger ones go straight to pageable memory.
+// Results that fit the thread's pinned staging buffer as it is come through
+// it (full-bandwidth copies, read in place by collect); others go straight to
+// pageable memory. The buffer is never grown for results: growing it frees
+// pinned memory, which synchronises the whole device and would stall every
+// other stream's work.
 int batch_fetch(Batch& b, cudaStream_t st, Pinned* pin = nullptr) {
     b.heads.resize(b.n_slots);
     b.best.resize(b.desc.size());
     const size_t hb = b.n_slots * sizeof(SlotHead), bb = b.desc.size() * sizeof(int2);
     const size_t pb = b.best_only ? b.desc.size() * (size_t)b.max_stride * 8 : (size_t)b.n_places * 8;
-    if (pin && hb + bb + pb <= (64u << 20) && pin->ensure(hb + bb + pb + 64) == cudaSuccess) {
+    if (pin && pin->p && hb + bb + pb <= pin->cap) {
         cudaError_t e = cudaMemcpyAsync(pin->p, b.d_mem + b.o_heads, hb, cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess)
             e = cudaMemcpyAsync(pin->p + hb, b.d_mem + b.o_best, bb, cudaMemcpyDeviceToHost, st);
@@ -798,8 +804,7 @@ int batch_fetch(Batch& b, cudaStream_t st, Pinned* pin = nullptr) {
         }
         std::memcpy(b.heads.data(), pin->p, hb);
         std::memcpy(b.best.data(), pin->p + hb, bb);
-        b.places.resize(std::max<size_t>(1, pb / 8));
-        std::memcpy(b.places.data(), pin->p + hb + bb, pb);
+        b.places_ptr = reinterpret_cast<const unsigned long long*>(pin->p + hb + bb);   // read in place
         return PLP_OK;
     }
     cudaError_t e = cudaMemcpyAsync(b.heads.data(), b.d_mem + b.o_heads, b.n_slots * sizeof(SlotHead),
@@ -819,6 +824,7 @@ int batch_fetch(Batch& b, cudaStream_t st, Pinned* pin = nullptr) {
         }
     }
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    b.places_ptr = b.places.data();
     if (e != cudaSuccess) {
         const int s = set_cuda_error("result copy", e);
         std::string keep = plpb_last();
@@ -875,12 +881,12 @@ std::vector<plp_result*> collect(const Batch& b, double time_s) {
         r->best_fallback = b.best[i].y;
         r->packed_slot.assign(d.restarts, -1);
         if (b.best_only) {
-            r->packed.assign(b.places.begin() + (long long)i * b.max_stride,
-                             b.places.begin() + (long long)i * b.max_stride + d.place_stride);
+            r->packed.assign(b.places_ptr + (long long)i * b.max_stride,
+                             b.places_ptr + (long long)i * b.max_stride + d.place_stride);
             if (r->best >= 0) r->packed_slot[r->best] = 0;
         } else {
-            r->packed.assign(b.places.begin() + d.place_off,
-                             b.places.begin() + d.place_off + (long long)d.restarts * d.place_stride);
+            r->packed.assign(b.places_ptr + d.place_off,
+                             b.places_ptr + d.place_off + (long long)d.restarts * d.place_stride);
             for (int k = 0; k < d.restarts; k++) r->packed_slot[k] = k;
         }
         out.push_back(r);
