@@ -427,8 +427,12 @@ struct Pinned {
     // whole host side)
     char* flag = nullptr;
     cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+    // outgrown buffers, freed with the context: freeing pinned memory
+    // synchronises the device, which would stall other streams mid-run
+    std::vector<char*> retired;
     ~Pinned() {
         if (p) cudaFreeHost(p);
+        for (char* q : retired) cudaFreeHost(q);
         if (flag) cudaFreeHost(flag);
         for (auto& e : ev)
             if (e) cudaEventDestroy(e);
@@ -442,7 +446,7 @@ struct Pinned {
     }
     cudaError_t ensure(size_t n) {
         if (n <= cap) return cudaSuccess;
-        if (p) cudaFreeHost(p);
+        if (p) retired.push_back(p);
         p = nullptr;
         cap = 0;
         size_t c = 1 << 20;
