@@ -88,10 +88,13 @@ void record(plp_handle* h, int status);
 // batch: device tables + one persistent decoder launch (+ retries)
 // ===========================================================================
 struct TileConfig {
-    int P = 128;       // placed-box tile depth per decoder
-    int C = 384;       // live-point tile depth per decoder
+    // default: the tile the autotuner picks on every bench workload (one
+    // decoder per CTA spreads a launch over all SMs; these depths hold the
+    // 400-item instances without capacity retries)
+    int P = 256;       // placed-box tile depth per decoder
+    int C = 512;       // live-point tile depth per decoder
     int G = 1;         // warps per decoder
-    int D = 8;         // decoders per CTA
+    int D = 1;         // decoders per CTA
     int M = 1;         // minimum resident CTAs per SM (register cap)
 };
 
