@@ -42,6 +42,7 @@ import plpb200 as P  # noqa: E402
 from plpb200 import synth  # noqa: E402
 
 REF_HARNESS = os.path.join(REPO, "oracle", "_ref", "ref_harness")
+REF_GPU = os.path.join(REPO, "oracle", "_ref", "plp_gpu_cuda")
 GOLDEN = os.path.join(REPO, "tests", "golden", "decoder.jsonl")
 PROFILE_INPUTS = os.path.join(REPO, "profiles", "roofline_inputs.txt")
 INT_OPS_PER_AABB = 6   # x, y, z interval tests of one AABB comparison
@@ -187,6 +188,32 @@ def cpu_baseline(insts, opts, R, threads):
     return out["decodes"] / out["seconds"], out, sample
 
 
+def reference_gpu(inst_py, opts):
+    """The reference's own CUDA build (gpu/plp_gpu.cu for sm_100a, built
+    under oracle/_ref) on the same instance: its --device K persistent kernel
+    at its K = 16 cap (time_s of the run, context set-up excluded), and its
+    plain one-launch-per-step path, as the rate difference of a 3 s and a
+    one-pass run, which cancels the CUDA context start-up."""
+    if not os.path.exists(REF_GPU):
+        return None
+    with tempfile.NamedTemporaryFile("w", suffix=".txt", delete=False) as f:
+        f.write(inst_py.to_thpack())
+        path = f.name
+    flags = ["--eps", str(opts.eps)] + (["--no-theta"] if math.isnan(opts.theta) else ["--theta", str(opts.theta)])
+    run = lambda extra: json.loads(subprocess.run([REF_GPU, path, "--json", "--seed", str(opts.seed)] + flags + extra,
+                                                  capture_output=True, text=True, check=True, timeout=120).stdout)
+    try:
+        dev = run(["--single-pass", "--device", "16"])
+        one = run(["--single-pass"])
+        many = run(["--time", "3"])
+    finally:
+        os.unlink(path)
+    plain = (many["n_passes"] - one["n_passes"]) / max(1e-9, many["time_s"] - one["time_s"])
+    return {"device_k16_decodes_per_s": 16 / dev["time_s"], "device_k16_ms_per_launch": 1000 * dev["time_s"],
+            "plain_decodes_per_s": plain,
+            "binary": "oracle/_ref/plp_gpu_cuda: the reference's gpu/plp_gpu.cu built for sm_100a"}
+
+
 def run_reference(args):
     """--impl reference: the reference's g++ decoder, all host threads."""
     rank = int(os.environ.get("RANK", "0"))
@@ -280,6 +307,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--no-reference-gpu", action="store_true")
     ap.add_argument("--tile", default=None,
                     help="P,C,G,D,M decoder tile instead of the autotuner's choice (profiling runs)")
     args = ap.parse_args()
@@ -407,6 +435,10 @@ def main():
                 cpu = {"value": v, "unit": "decodes/s", "cores": raw["threads"], "kind": "reference",
                        "sample": f"{sample} restarts x 4 repeats of the workload's first instance, reference "
                                  f"g++ build of gpu/plp_common.hpp, {raw['threads']} threads"}
+                one = cpu_baseline(insts_py, opts, min(R, 128), 1)
+                if one:
+                    cpu["single_core"] = {"value": one[0], "unit": "decodes/s",
+                                          "sample": f"{one[2]} restarts x 4 repeats, 1 thread"}
         plain = None
         if not args.no_plain:
             n_pl = 8
@@ -422,6 +454,9 @@ def main():
                      "feasibility launch per item step (plp_run_plain)", "speedup_of_persistent": value / world / pv}
             del o_pl
         serving = None if args.no_serving else serving_report(local)
+        ref_gpu = None
+        if not args.no_reference_gpu and args.workload == "multi_restart":
+            ref_gpu = reference_gpu(insts_py[0], opts)
         out = {
             "metric": "decodes/sec", "value": value, "unit": "decodes/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
@@ -440,6 +475,7 @@ def main():
             "roofline": roofline,
             "cpu_baseline": cpu,
             "plain_path": plain,
+            "reference_gpu": ref_gpu,
             "serving": serving,
             "clocks": clk,
         }
