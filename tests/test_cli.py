@@ -181,3 +181,21 @@ def test_multi_instance_file_in_one_launch(extra):
             assert a == b
             if "--device" not in extra:
                 assert a == _ref([one, "--json", "--seed", "2", "--single-pass"])
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not os.path.exists(os.path.join(O.REF_DIR, "plp_gpu_cuda")),
+                    reason="reference CUDA build not present")
+@pytest.mark.parametrize("flags", [["--single-pass"], ["--single-pass", "--eps", "0", "--no-theta"]])
+def test_reference_cuda_build_rows_equal_ours(inst_file, flags):
+    """The reference's own CUDA build (--device K, its persistent kernel) on
+    the same GPU gives the rows this library gives."""
+    ref = subprocess.run([os.path.join(O.REF_DIR, "plp_gpu_cuda"), inst_file, "--device", "8", "--json",
+                          "--seed", "4"] + flags, capture_output=True, text=True, check=True, timeout=300)
+    ours = run([inst_file, "--device", "8", "--json", "--seed", "4"] + flags)
+    assert ours.returncode == 0
+    a, b = json.loads(ref.stdout)["rows"], json.loads(ours.stdout)["rows"]
+    for x, y in zip(a, b):
+        x.pop("time_s")
+        y.pop("time_s")
+    assert a == b and len(a) == 8
