@@ -240,6 +240,10 @@ struct Batch {
     bool multi_pass = false;
     // block-building engine: shape catalogue and per-instance orderings
     int engine = 0, max_types = 0;
+    // contact areas of the decoder in 16 bits: allowed when every
+    // orientation's footprint area is below 65536, chosen (plan) when the
+    // batch's restarts exceed one wave at 32-bit residency
+    int sup16_ok = 1, sup16 = 0;
     std::vector<BlkShape> bcat;
     std::vector<int> btab;
     // device
@@ -278,6 +282,8 @@ struct Batch {
         bcat.clear(); btab.clear();
         engine = op.empty() ? 0 : op[0].engine;
         max_types = 0;
+        sup16_ok = 1;
+        sup16 = 0;
         n_slots = 0; n_places = 0; max_stride = 1; max_steps = 0; multi_pass = false;
         int maxH = 0;
         best_only = true;
@@ -332,6 +338,8 @@ struct Batch {
                 const auto v = orientations(t);
                 to.n = (int)v.size();
                 for (int k = 0; k < to.n; k++) { to.w[k] = v[k][0]; to.d[k] = v[k][1]; to.h[k] = v[k][2]; }
+                for (int k = 0; k < to.n; k++)
+                    if (1LL * to.w[k] * to.d[k] >= 65536) sup16_ok = 0;
                 ot.push_back(to);
                 types.push_back(to);
             }
@@ -371,6 +379,14 @@ struct Batch {
 
     void plan(int sms, const TileConfig& t) {
         tile = t;
+        // a latency-bound launch (one wave) gains nothing from the smaller
+        // footprint and the 32-bit areas are a little faster to update
+        sup16 = 0;
+        if (engine == 0 && sup16_ok && t.G == 1) {
+            int occ32 = 1;
+            if (tile_occupancy(*this, t, &occ32) != cudaSuccess || occ32 < 1) occ32 = 1;
+            sup16 = n_slots > (long long)sms * occ32 * t.D ? 1 : 0;
+        }
         int occ = 1;
         if (tile_occupancy(*this, t, &occ) != cudaSuccess || occ < 1) occ = 1;
         const long long need = (n_slots + t.D - 1) / t.D;
@@ -398,7 +414,7 @@ struct Batch {
 
 int tile_smem(const Batch& b, const TileConfig& t) {
     return b.engine == 1 ? block_smem_bytes(t.P, t.C, std::max(1, b.max_steps), std::max(1, b.max_types), b.Hz)
-                         : decoder_smem_bytes(t.P, t.C, b.Hz, t.G);
+                         : decoder_smem_bytes(t.P, t.C, b.Hz, t.G, b.sup16);
 }
 
 bool tile_supported(const Batch& b, const TileConfig& t) {
@@ -408,7 +424,7 @@ bool tile_supported(const Batch& b, const TileConfig& t) {
 cudaError_t tile_occupancy(const Batch& b, const TileConfig& t, int* occ) {
     if (b.engine == 1)
         return block_occupancy(t.P, t.C, std::max(1, b.max_steps), std::max(1, b.max_types), b.Hz, t.D, t.M, occ);
-    return decoder_occupancy(t.P, t.C, b.Hz, t.G, t.D, t.M, occ);
+    return decoder_occupancy(t.P, t.C, b.Hz, t.G, t.D, t.M, occ, b.sup16);
 }
 
 // Fewer decoders per CTA when the tile plus this batch's top-z index (and,
@@ -573,6 +589,7 @@ static DecodeLaunch make_launch(const Batch& b, const TileConfig& t, const int2*
     L.C = t.C;
     L.Hz = b.Hz;
     L.engine = b.engine;
+    L.sup16 = b.sup16;
     L.bcat = reinterpret_cast<const BlkShape*>(b.d_mem + b.o_bcat);
     L.btab = reinterpret_cast<const int*>(b.d_mem + b.o_btab);
     L.N = std::max(1, b.max_steps);

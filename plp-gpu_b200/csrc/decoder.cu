@@ -53,6 +53,7 @@
 #include <climits>
 #include <cstdio>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 namespace plpb {
@@ -113,7 +114,10 @@ struct Dec1Layout {
     int off_bx, off_bz, off_z2, off_bi, off_key, off_st, off_sup, off_w, off_wi, off_zt, off_sh, bytes;
 };
 
-__host__ __device__ inline Dec1Layout dec1_layout(int P, int C, int Hz) {
+// sb: bytes per stored contact area (4, or 2 when every orientation's
+// footprint area is below 65536; an area never exceeds its footprint, since
+// boxes sharing a top cannot overlap below it)
+__host__ __device__ inline Dec1Layout dec1_layout(int P, int C, int Hz, int sb) {
     Dec1Layout l;
     int o = 624 * 4;                       // MT state
     o = (o + 15) & ~15;
@@ -126,7 +130,7 @@ __host__ __device__ inline Dec1Layout dec1_layout(int P, int C, int Hz) {
     l.off_key = o;
     l.off_st = o + 4 * C;
     l.off_sup = o + 8 * C;
-    int region = 32 * C;
+    int region = (8 + 6 * sb) * C;
     if (region < 18 * P + 32) region = 18 * P + 32;
     o += region;
     o = (o + 15) & ~15;
@@ -140,8 +144,8 @@ __host__ __device__ inline Dec1Layout dec1_layout(int P, int C, int Hz) {
     return l;
 }
 
-int decoder_smem_bytes(int P, int C, int Hz, int G) {
-    return G == 1 ? dec1_layout(P, C, Hz).bytes : dec_layout(P, C, Hz).bytes;
+int decoder_smem_bytes(int P, int C, int Hz, int G, int sup16) {
+    return G == 1 ? dec1_layout(P, C, Hz, sup16 ? 2 : 4).bytes : dec_layout(P, C, Hz).bytes;
 }
 
 struct DecoderArgs {
@@ -790,10 +794,11 @@ __device__ __forceinline__ unsigned st_feasible(uint32_t s) {
 // items at a time, lg chosen so that a short item list still spreads over the
 // whole warp. Greedy mode stops after the first group holding a feasible
 // item. Returns {first feasible item or INT_MAX, end of the evaluated range}.
+template <typename SupT>
 __device__ __forceinline__ int2 eval_items(const bool GREEDY, const uint2* W, const unsigned short* wi, int w0, int w1,
                                            const int4* bx, const int* bzs, int nb, const StepOrs& S,
                                            uint32_t xmask, uint32_t ymask, int xb, int xyb,
-                                           uint32_t* st, int* sup, int C, int lane) {
+                                           uint32_t* st, SupT* sup, int C, int lane) {
     int first = INT_MAX;
     int w = w0;
     while (w < w1) {
@@ -894,12 +899,12 @@ __device__ __forceinline__ int2 eval_items(const bool GREEDY, const uint2* W, co
             const int p = wi[w + q];
             st[p] = st_pack(m2, known & ~alive, sok, known);
             if (z > 0) {
-                sup[p] = a0;
-                sup[C + p] = a1;
-                sup[2 * C + p] = a2;
-                sup[3 * C + p] = a3;
-                sup[4 * C + p] = a4;
-                sup[5 * C + p] = a5;
+                sup[p] = (SupT)a0;
+                sup[C + p] = (SupT)a1;
+                sup[2 * C + p] = (SupT)a2;
+                sup[3 * C + p] = (SupT)a3;
+                sup[4 * C + p] = (SupT)a4;
+                sup[5 * C + p] = (SupT)a5;
             }
         }
         w += K;
@@ -918,8 +923,9 @@ __device__ __forceinline__ int2 eval_items(const bool GREEDY, const uint2* W, co
 // Applies one newly placed box to a valid point's state (C1 OR, C3 contact
 // areas). Returns the new state, or 0 when the support grew onto an
 // orientation whose C1 was never evaluated (the point is re-evaluated).
+template <typename SupT>
 __device__ __forceinline__ uint32_t st_apply_box(uint32_t s, int x, int y, int z, int4 B, int Bz, int Bz2,
-                                                 const StepOrs& S, int* sup, int C, int p) {
+                                                 const StepOrs& S, SupT* sup, int C, int p) {
     const unsigned m2 = s & 0x3fu, known = (s >> 24) & 0x3fu;
     unsigned blk = (s >> 8) & 0x3fu, sok = (s >> 16) & 0x3fu;
     if (Bz2 > z && x < B.z && y < B.w) {
@@ -934,8 +940,8 @@ __device__ __forceinline__ uint32_t st_apply_box(uint32_t s, int x, int y, int z
                 const int ox = min(x + S.ow[o], B.z) - max(x, B.x);
                 const int oy = min(y + S.od[o], B.w) - max(y, B.y);
                 if (ox > 0 && oy > 0) {
-                    const int v = sup[o * C + p] + ox * oy;
-                    sup[o * C + p] = v;
+                    const int v = (int)sup[o * C + p] + ox * oy;
+                    sup[o * C + p] = (SupT)v;
                     if (2LL * v >= (long long)S.wd[o]) sok |= 1u << o;
                 }
             }
@@ -948,8 +954,9 @@ __device__ __forceinline__ uint32_t st_apply_box(uint32_t s, int x, int y, int z
 // Warp: pick the pair, place the box, drop the points it covers and insert
 // its uncovered corners (invalid), then update the top-sorted box tables and
 // the top-z index. pp is the first point holding a feasible pair.
+template <typename SupT>
 __device__ __forceinline__ int place1(int t, int pp, bool full, uint32_t* mt, int& mpos, uint32_t* keys,
-                                      uint32_t* st, int* sup, int4* bx, int* bzs, int* z2s,
+                                      uint32_t* st, SupT* sup, int4* bx, int* bzs, int* z2s,
                                       unsigned short* bis, unsigned short* zt, int Hz, int& nc, int& nb,
                                       int P, int C, const StepOrs& S, uint32_t xmask, uint32_t ymask,
                                       int xb, int xyb, unsigned long long* pass_out, long long& vol,
@@ -1077,8 +1084,8 @@ __device__ __forceinline__ int place1(int t, int pp, bool full, uint32_t* mt, in
                 keys[d] = key;
                 st[d] = s;
                 if (mv_sup) {
-                    sup[d] = s0; sup[C + d] = s1; sup[2 * C + d] = s2;
-                    sup[3 * C + d] = s3; sup[4 * C + d] = s4; sup[5 * C + d] = s5;
+                    sup[d] = (SupT)s0; sup[C + d] = (SupT)s1; sup[2 * C + d] = (SupT)s2;
+                    sup[3 * C + d] = (SupT)s3; sup[4 * C + d] = (SupT)s4; sup[5 * C + d] = (SupT)s5;
                 }
             }
         }
@@ -1136,8 +1143,8 @@ __device__ __forceinline__ int place1(int t, int pp, bool full, uint32_t* mt, in
                 keys[d] = key;
                 st[d] = s;
                 if (mv_sup) {
-                    sup[d] = s0; sup[C + d] = s1; sup[2 * C + d] = s2;
-                    sup[3 * C + d] = s3; sup[4 * C + d] = s4; sup[5 * C + d] = s5;
+                    sup[d] = (SupT)s0; sup[C + d] = (SupT)s1; sup[2 * C + d] = (SupT)s2;
+                    sup[3 * C + d] = (SupT)s3; sup[4 * C + d] = (SupT)s4; sup[5 * C + d] = (SupT)s5;
                 }
             }
             __syncwarp();
@@ -1156,9 +1163,10 @@ __device__ __forceinline__ int place1(int t, int pp, bool full, uint32_t* mt, in
     return ERR_NONE;
 }
 
+template <typename SupT>
 __device__ __forceinline__ void decoder1_body(const DecoderArgs& a, unsigned char* base, int gdec) {
     const int lane = threadIdx.x & 31;
-    const Dec1Layout lay = dec1_layout(a.P, a.C, a.Hz);
+    const Dec1Layout lay = dec1_layout(a.P, a.C, a.Hz, (int)sizeof(SupT));
     const int C = a.C;
     uint32_t* mt = reinterpret_cast<uint32_t*>(base);
     int4* bx = reinterpret_cast<int4*>(base + lay.off_bx);
@@ -1167,7 +1175,7 @@ __device__ __forceinline__ void decoder1_body(const DecoderArgs& a, unsigned cha
     unsigned short* bis = reinterpret_cast<unsigned short*>(base + lay.off_bi);
     uint32_t* keys = reinterpret_cast<uint32_t*>(base + lay.off_key);
     uint32_t* st = reinterpret_cast<uint32_t*>(base + lay.off_st);
-    int* sup = reinterpret_cast<int*>(base + lay.off_sup);
+    SupT* sup = reinterpret_cast<SupT*>(base + lay.off_sup);
     uint2* Wl = reinterpret_cast<uint2*>(base + lay.off_w);
     unsigned short* wi = reinterpret_cast<unsigned short*>(base + lay.off_wi);
     unsigned short* zt = a.Hz ? reinterpret_cast<unsigned short*>(base + lay.off_zt) : nullptr;
@@ -1354,12 +1362,14 @@ __device__ __forceinline__ void decoder1_body(const DecoderArgs& a, unsigned cha
     }
 }
 
-template <int D, int M>
+// S16: contact areas stored as 16-bit (every footprint area < 65536)
+template <int D, int M, int S16>
 __global__ void __launch_bounds__(32 * D, M) decoder1_kernel(DecoderArgs a) {
+    using SupT = typename std::conditional<S16 != 0, unsigned short, int>::type;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int dec = threadIdx.x >> 5;
-    const Dec1Layout lay = dec1_layout(a.P, a.C, a.Hz);
-    decoder1_body(a, smem_raw + (size_t)dec * lay.bytes, blockIdx.x * D + dec);
+    const Dec1Layout lay = dec1_layout(a.P, a.C, a.Hz, (int)sizeof(SupT));
+    decoder1_body<SupT>(a, smem_raw + (size_t)dec * lay.bytes, blockIdx.x * D + dec);
 }
 
 // ---------------------------------------------------------------------------
@@ -1548,16 +1558,17 @@ __global__ void gather_best_kernel(const InstDesc* __restrict__ inst, int n_inst
 
 using DecoderFn = void (*)(DecoderArgs);
 
-// G = 1: the incremental single-warp decoder; G > 1: the multi-warp decoder
+// G = 1: the incremental single-warp decoder (16- or 32-bit contact areas);
+// G > 1: the multi-warp decoder
 template <int G, int D, int M>
-static DecoderFn pick_kernel() {
-    if constexpr (G == 1) return decoder1_kernel<D, M>;
+static DecoderFn pick_kernel(int sup16) {
+    if constexpr (G == 1) return sup16 ? decoder1_kernel<D, M, 1> : decoder1_kernel<D, M, 0>;
     else return decoder_kernel<G, D, M>;
 }
 
-static DecoderFn decoder_fn(int G, int D, int M) {
+static DecoderFn decoder_fn(int G, int D, int M, int sup16 = 0) {
 #define PLP_PICK(g, d, m) \
-    if (G == g && D == d && M == m) return pick_kernel<g, d, m>();
+    if (G == g && D == d && M == m) return pick_kernel<g, d, m>(sup16);
     PLP_DECODER_CONFIGS(PLP_PICK)
 #undef PLP_PICK
     return nullptr;
@@ -1586,14 +1597,14 @@ static DecoderArgs decoder_args(const DecodeLaunch& L) {
 }
 
 static int decoder_launch_smem(const DecodeLaunch& L) {
-    return decoder_smem_bytes(L.P, L.C, L.Hz, L.warps_per_decoder) * L.decoders_per_cta;
+    return decoder_smem_bytes(L.P, L.C, L.Hz, L.warps_per_decoder, L.sup16) * L.decoders_per_cta;
 }
 
 // Function attributes (dynamic shared memory) for a launch; not a stream
 // operation, so it is done before any capture.
 cudaError_t configure_decoder(const DecodeLaunch& L) {
     if (L.engine == 1) return configure_block(L);
-    DecoderFn fn = decoder_fn(L.warps_per_decoder, L.decoders_per_cta, L.min_blocks);
+    DecoderFn fn = decoder_fn(L.warps_per_decoder, L.decoders_per_cta, L.min_blocks, L.sup16);
     if (!fn) return cudaErrorInvalidConfiguration;
     return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, decoder_launch_smem(L));
 }
@@ -1601,7 +1612,7 @@ cudaError_t configure_decoder(const DecodeLaunch& L) {
 // Stream operations only (counter resets and the launch): capturable.
 cudaError_t enqueue_decoder(const DecodeLaunch& L, cudaStream_t st) {
     if (L.engine == 1) return enqueue_block(L, st);
-    DecoderFn fn = decoder_fn(L.warps_per_decoder, L.decoders_per_cta, L.min_blocks);
+    DecoderFn fn = decoder_fn(L.warps_per_decoder, L.decoders_per_cta, L.min_blocks, L.sup16);
     if (!fn) return cudaErrorInvalidConfiguration;
     cudaError_t e = cudaMemsetAsync(L.work_next, 0, sizeof(int), st);
     if (e != cudaSuccess) return e;
@@ -1617,10 +1628,10 @@ cudaError_t launch_decoder(const DecodeLaunch& L, cudaStream_t st) {
     return enqueue_decoder(L, st);
 }
 
-cudaError_t decoder_occupancy(int P, int C, int Hz, int G, int D, int M, int* ctas_per_sm) {
-    DecoderFn fn = decoder_fn(G, D, M);
+cudaError_t decoder_occupancy(int P, int C, int Hz, int G, int D, int M, int* ctas_per_sm, int sup16) {
+    DecoderFn fn = decoder_fn(G, D, M, sup16);
     if (!fn) return cudaErrorInvalidConfiguration;
-    const int smem = decoder_smem_bytes(P, C, Hz, G) * D;
+    const int smem = decoder_smem_bytes(P, C, Hz, G, sup16) * D;
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas_per_sm, fn, 32 * G * D, smem);

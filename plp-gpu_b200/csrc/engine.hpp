@@ -23,6 +23,7 @@ struct DecodeLaunch {
     int P, C;                 // shared-memory tile: boxes and live points per decoder
     int Hz;                   // entries of the top-z index (max height + 2), 0 = none
     int engine;               // 0 extreme-point decoder, 1 block-building engine
+    int sup16;                // decoder: contact areas stored as 16-bit
     const BlkShape* bcat;     // block engine: shape catalogue of the batch
     const int* btab;          // block engine: per-instance orderings (ints)
     int N, T;                 // block engine tile: items, types per decoder
@@ -32,9 +33,9 @@ struct DecodeLaunch {
     int ctas;
 };
 
-int decoder_smem_bytes(int P, int C, int Hz, int G);
+int decoder_smem_bytes(int P, int C, int Hz, int G, int sup16 = 0);   // sup16: 16-bit contact areas
 bool decoder_config_supported(int G, int D, int M);
-cudaError_t decoder_occupancy(int P, int C, int Hz, int G, int D, int M, int* ctas_per_sm);
+cudaError_t decoder_occupancy(int P, int C, int Hz, int G, int D, int M, int* ctas_per_sm, int sup16 = 0);
 cudaError_t launch_decoder(const DecodeLaunch& L, cudaStream_t st);     // configure + enqueue
 cudaError_t configure_decoder(const DecodeLaunch& L);                    // function attributes
 cudaError_t enqueue_decoder(const DecodeLaunch& L, cudaStream_t st);     // stream operations only

@@ -219,3 +219,17 @@ def test_time_budget_pass_cap_binds():
         f = h.solve([inst], P.make_opts(seed=1, restarts=8, passes=3))[0]
     assert [r.summary(k).n_passes for k in range(8)] == [3] * 8
     assert _jsons(r) == _jsons(f)
+
+
+def test_multi_wave_batch_matches_oracle():
+    """A batch larger than one wave of resident decoders (3000 restarts) runs
+    with the contact areas in 16 bits; a stride sample against the oracle."""
+    texts = [i.to_thpack() for i in synth.batched_set(60, 35000)]
+    insts = [P.Instance.parse(t) for t in texts]
+    with P.Handle() as h:
+        res = h.solve(insts, P.make_opts(seed=20, restarts=50))
+    for n, (t, r) in enumerate(zip(texts, res)):
+        oi = O.OInstance(t)
+        for k in range((n * 7) % 13, 50, 13):
+            js, _, _ = O.run(oi, seed=20 + k)
+            assert O.strip_time(r.json(k)) == O.strip_time(js), (n, k)

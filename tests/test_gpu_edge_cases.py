@@ -33,6 +33,9 @@ CASES = {
                                                           (35, 1, 25, 0, 15, 1, 9), (60, 1, 45, 1, 30, 1, 5)]),
     "single_item": thpack(300, 200, 100, [(80, 1, 60, 1, 40, 1, 1)]),
     "one_long_run": thpack(400, 250, 200, [(37, 1, 29, 1, 23, 1, 180)]),
+    # footprints of 300 x 300 >= 65536: contact areas stay 32-bit
+    "large_footprints_32bit_areas": thpack(1000, 1000, 100, [(300, 1, 300, 1, 40, 1, 9), (250, 1, 180, 1, 30, 1, 14),
+                                                             (90, 1, 70, 1, 20, 1, 30)]),
 }
 
 
