@@ -15,8 +15,11 @@
 #include <map>
 #include <memory>
 #include <mutex>
+#include <new>
 #include <thread>
 #include <unordered_map>
+
+#include <unistd.h>
 
 #include "capi_internal.hpp"
 #include "engine.hpp"
@@ -264,12 +267,13 @@ struct Batch {
     cudaGraphExec_t gexec = nullptr;
     TileConfig gtile;
     int glaunches = 0;
-    // host results
-    std::vector<SlotHead> heads;
-    std::vector<int2> best;
-    std::vector<unsigned long long> places;   // all slots, or gathered best per instance
-    // where the fetched placements are: places.data(), or the fetching
-    // thread's pinned staging buffer (valid until that thread's next batch)
+    // host results: one block of [slot heads | best per instance | packed
+    // placements (all slots, or the gathered best per instance)], shared
+    // with the result objects that read it in place
+    std::vector<SlotHead> heads;              // scratch of the capacity-retry loop
+    std::shared_ptr<char> host;
+    const SlotHead* heads_ptr = nullptr;
+    const int2* best_ptr = nullptr;
     const unsigned long long* places_ptr = nullptr;
     bool best_only = false;
     double t_start = 0, t_end = 0;
@@ -475,6 +479,71 @@ struct Pinned {
         return e;
     }
 };
+
+// Pinned host blocks that the results of synchronous solves are read from in
+// place: the device writes each result byte once, into memory the result
+// objects keep. A block returns to the free list when the last result
+// viewing it is freed, and the pool pins at most `limit` bytes (a solve that
+// finds no room copies into pageable memory instead). Pinned memory is freed
+// only when the pool is destroyed with its handle: freeing it synchronises
+// the device.
+struct HostPool {
+    std::mutex mu;
+    std::vector<std::pair<char*, size_t>> free_list;   // (block, capacity)
+    size_t held = 0;
+    size_t limit = 0;
+    HostPool() {
+        const long pages = sysconf(_SC_PHYS_PAGES), page = sysconf(_SC_PAGESIZE);
+        const size_t phys = pages > 0 && page > 0 ? (size_t)pages * (size_t)page : ((size_t)16 << 30);
+        limit = std::min((size_t)8 << 30, phys / 4);
+    }
+    ~HostPool() {
+        for (auto& f : free_list) cudaFreeHost(f.first);
+    }
+};
+
+// a block of at least n bytes from the pool, or null when the pool is full
+std::shared_ptr<char> pool_take(const std::shared_ptr<HostPool>& pool, size_t n) {
+    n = std::max<size_t>(n, 1);
+    size_t cap = (size_t)1 << 20;             // 1 MiB, then 1/8-power-of-two steps
+    while (cap < n) cap <<= 1;
+    if (cap > ((size_t)8 << 20)) {
+        const size_t step = cap >> 3;
+        cap = (n + step - 1) / step * step;
+    }
+    char* p = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(pool->mu);
+        int pick = -1;
+        for (size_t i = 0; i < pool->free_list.size(); i++)
+            if (pool->free_list[i].second >= n &&
+                (pick < 0 || pool->free_list[i].second < pool->free_list[pick].second))
+                pick = (int)i;
+        if (pick >= 0) {
+            p = pool->free_list[pick].first;
+            cap = pool->free_list[pick].second;
+            pool->free_list.erase(pool->free_list.begin() + pick);
+        } else {
+            if (pool->held + cap > pool->limit) return nullptr;
+            pool->held += cap;                // reserved; allocated outside the lock
+        }
+    }
+    if (!p && cudaMallocHost(&p, cap) != cudaSuccess) {
+        cudaGetLastError();
+        std::lock_guard<std::mutex> lk(pool->mu);
+        pool->held -= cap;
+        return nullptr;
+    }
+    std::weak_ptr<HostPool> wp = pool;
+    return std::shared_ptr<char>(p, [wp, cap](char* q) {
+        if (auto sp = wp.lock()) {
+            std::lock_guard<std::mutex> lk(sp->mu);
+            sp->free_list.push_back({q, cap});
+        } else {
+            cudaFreeHost(q);
+        }
+    });
+}
 
 }  // namespace
 
@@ -806,49 +875,32 @@ int batch_execute(Batch& b, cudaStream_t st, int sms, TileConfig& tile, ExecStat
 // pageable memory. The buffer is never grown for results: growing it frees
 // pinned memory, which synchronises the whole device and would stall every
 // other stream's work.
-int batch_fetch(Batch& b, cudaStream_t st, Pinned* pin = nullptr) {
-    b.heads.resize(b.n_slots);
-    b.best.resize(b.desc.size());
+// Copies a finished batch's results to the host. With a pool the copies land
+// in a pooled pinned block that the results keep; else in a pageable block,
+// staged through the thread's pinned buffer when it is large enough (the
+// staging buffer is reused by the thread's next batch, so it is copied out).
+int batch_fetch(Batch& b, cudaStream_t st, Pinned* pin = nullptr, const std::shared_ptr<HostPool>* pool = nullptr) {
     const size_t hb = b.n_slots * sizeof(SlotHead), bb = b.desc.size() * sizeof(int2);
     const size_t pb = b.best_only ? b.desc.size() * (size_t)b.max_stride * 8 : (size_t)b.n_places * 8;
-    if (pin && pin->p && hb + bb + pb <= pin->cap) {
-        cudaError_t e = cudaMemcpyAsync(pin->p, b.d_mem + b.o_heads, hb, cudaMemcpyDeviceToHost, st);
-        if (e == cudaSuccess)
-            e = cudaMemcpyAsync(pin->p + hb, b.d_mem + b.o_best, bb, cudaMemcpyDeviceToHost, st);
-        if (e == cudaSuccess && pb)
-            e = cudaMemcpyAsync(pin->p + hb + bb, b.d_mem + (b.best_only ? b.o_gather : b.o_places), pb,
-                                cudaMemcpyDeviceToHost, st);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-        if (e != cudaSuccess) {
-            const int s = set_cuda_error("result copy", e);
-            std::string keep = plpb_last();
+    const size_t total = hb + bb + pb;
+    std::shared_ptr<char> blk;
+    if (pool && *pool) blk = pool_take(*pool, total);
+    char* stage = nullptr;
+    if (!blk) {
+        if (pin && pin->p && total <= pin->cap) stage = pin->p;
+        blk = std::shared_ptr<char>(new (std::nothrow) char[std::max<size_t>(total, 1)], std::default_delete<char[]>());
+        if (!blk) {
             batch_release(b, st);
-            set_error(s, keep);
-            return s;
+            return set_error(PLP_E_CAPACITY, "host memory for the results could not be allocated");
         }
-        std::memcpy(b.heads.data(), pin->p, hb);
-        std::memcpy(b.best.data(), pin->p + hb, bb);
-        b.places_ptr = reinterpret_cast<const unsigned long long*>(pin->p + hb + bb);   // read in place
-        return PLP_OK;
     }
-    cudaError_t e = cudaMemcpyAsync(b.heads.data(), b.d_mem + b.o_heads, b.n_slots * sizeof(SlotHead),
-                                    cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess)
-        e = cudaMemcpyAsync(b.best.data(), b.d_mem + b.o_best, b.desc.size() * sizeof(int2),
+    char* dst = stage ? stage : blk.get();
+    cudaError_t e = cudaMemcpyAsync(dst, b.d_mem + b.o_heads, hb, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dst + hb, b.d_mem + b.o_best, bb, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess && pb)
+        e = cudaMemcpyAsync(dst + hb + bb, b.d_mem + (b.best_only ? b.o_gather : b.o_places), pb,
                             cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess) {
-        if (b.best_only) {
-            b.places.resize(b.desc.size() * (size_t)b.max_stride);
-            e = cudaMemcpyAsync(b.places.data(), b.d_mem + b.o_gather, b.places.size() * 8,
-                                cudaMemcpyDeviceToHost, st);
-        } else {
-            b.places.resize((size_t)std::max<long long>(1, b.n_places));
-            e = cudaMemcpyAsync(b.places.data(), b.d_mem + b.o_places, b.n_places * 8,
-                                cudaMemcpyDeviceToHost, st);
-        }
-    }
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    b.places_ptr = b.places.data();
     if (e != cudaSuccess) {
         const int s = set_cuda_error("result copy", e);
         std::string keep = plpb_last();
@@ -856,6 +908,11 @@ int batch_fetch(Batch& b, cudaStream_t st, Pinned* pin = nullptr) {
         set_error(s, keep);
         return s;
     }
+    if (stage) std::memcpy(blk.get(), stage, total);
+    b.host = std::move(blk);
+    b.heads_ptr = reinterpret_cast<const SlotHead*>(b.host.get());
+    b.best_ptr = reinterpret_cast<const int2*>(b.host.get() + hb);
+    b.places_ptr = reinterpret_cast<const unsigned long long*>(b.host.get() + hb + bb);
     return PLP_OK;
 }
 
@@ -867,19 +924,22 @@ size_t batch_d2h_bytes(const Batch& b) {
 }
 
 // full synchronous run used by plp_solve and the serving workers
-int run_batch(Batch& b, cudaStream_t st, Pinned& pin, int sms, TileConfig& tile) {
+int run_batch(Batch& b, cudaStream_t st, Pinned& pin, int sms, TileConfig& tile,
+              const std::shared_ptr<HostPool>* pool = nullptr) {
     int s = batch_prepare(b, st, pin, sms, tile, true);
     if (s != PLP_OK) return s;
     s = batch_execute(b, st, sms, tile, nullptr, false);
     if (s != PLP_OK) return s;
-    s = batch_fetch(b, st, &pin);
+    s = batch_fetch(b, st, &pin, pool);
     if (s != PLP_OK) return s;
     return batch_release(b, st);
 }
 
-// Builds the per-instance result objects of a finished batch.
+// Builds the per-instance result objects of a finished batch; they view the
+// batch's host block in place.
 std::vector<plp_result*> collect(const Batch& b, double time_s) {
     std::vector<plp_result*> out;
+    out.reserve(b.desc.size());
     for (size_t i = 0; i < b.desc.size(); i++) {
         const InstDesc& d = b.desc[i];
         auto* r = new plp_result;
@@ -888,31 +948,14 @@ std::vector<plp_result*> collect(const Batch& b, double time_s) {
         r->ors = b.inst_ors[i];
         r->L = d.L; r->W = d.W; r->H = d.H;
         r->steps.assign(b.steps.begin() + d.step_off, b.steps.begin() + d.step_off + d.n_steps);
-        r->summ.resize(d.restarts);
-        for (int k = 0; k < d.restarts; k++) {
-            const SlotHead& h = b.heads[d.slot_base + k];
-            plp_summary& s = r->summ[k];
-            s.n_boxes = h.n_boxes;
-            s.fallback = h.fallback;
-            s.volume = h.volume;
-            s.score = h.score;
-            s.n_passes = h.n_passes;
-            s.err = h.err;
-            s.seed = d.seed + k;
-            s.time_s = time_s;
-        }
-        r->best = b.best[i].x;
-        r->best_fallback = b.best[i].y;
-        r->packed_slot.assign(d.restarts, -1);
-        if (b.best_only) {
-            r->packed.assign(b.places_ptr + (long long)i * b.max_stride,
-                             b.places_ptr + (long long)i * b.max_stride + d.place_stride);
-            if (r->best >= 0) r->packed_slot[r->best] = 0;
-        } else {
-            r->packed.assign(b.places_ptr + d.place_off,
-                             b.places_ptr + d.place_off + (long long)d.restarts * d.place_stride);
-            for (int k = 0; k < d.restarts; k++) r->packed_slot[k] = k;
-        }
+        r->block = b.host;
+        r->heads = b.heads_ptr + d.slot_base;
+        r->seed0 = d.seed;
+        r->time_s = time_s;
+        r->best = b.best_ptr[i].x;
+        r->best_fallback = b.best_ptr[i].y;
+        r->kept_all = !b.best_only;
+        r->packed = b.places_ptr + (b.best_only ? (long long)i * b.max_stride : d.place_off);
         out.push_back(r);
     }
     return out;
@@ -957,6 +1000,7 @@ struct plp_handle {
     cudaStream_t sync_stream = nullptr;
     std::mutex sync_mu;
     Pinned sync_pin;
+    std::shared_ptr<HostPool> pool = std::make_shared<HostPool>();   // result blocks of synchronous solves
 };
 
 namespace {
@@ -1195,7 +1239,7 @@ int32_t plp_result_restarts(const plp_result* r) { return r ? r->restarts : 0; }
 int plp_result_summary(const plp_result* r, int32_t k, plp_summary* out) {
     if (!r || !out) return set_error(PLP_E_INVALID, "plp_result_summary: null argument");
     if (k < 0 || k >= r->restarts) return set_error(PLP_E_INVALID, "restart out of range");
-    *out = r->summ[k];
+    *out = r->summary(k);
     return PLP_OK;
 }
 
@@ -1205,9 +1249,9 @@ static int expand(const plp_result* r, int k, std::vector<Placement>& v) {
         v.assign(r->rows.begin() + r->row_off[k], r->rows.begin() + r->row_off[k + 1]);
         return PLP_OK;
     }
-    const int slot = r->packed_slot[k];
+    const int slot = r->packed_slot(k);
     if (slot < 0) return set_error(PLP_E_NOT_FOUND, "placements of this restart were not kept (best_only)");
-    const int n = r->summ[k].n_boxes;
+    const int n = r->heads[k].n_boxes;
     for (int i = 0; i < n; i++) {
         int x, y, z, oi, t;
         unpack_place(r->packed[(size_t)slot * r->stride + i], x, y, z, oi, t);
@@ -1247,7 +1291,7 @@ int plp_result_json(const plp_result* r, int32_t k, char* buf, size_t cap, size_
     std::vector<Placement> v;
     int s = expand(r, k, v);
     if (s != PLP_OK) return s;
-    const plp_summary& S = r->summ[k];
+    const plp_summary S = r->summary(k);
     RunSummary rs;
     rs.n_boxes = S.n_boxes;
     rs.volume = S.volume;
@@ -1515,7 +1559,7 @@ int plp_solve(plp_handle* h, const plp_instance* const* insts, int32_t n_inst,
         std::lock_guard<std::mutex> lk(h->mu);
         tile = h->tile;
     }
-    if (s == PLP_OK) s = run_batch(b, h->sync_stream, h->sync_pin, h->sms, tile);
+    if (s == PLP_OK) s = run_batch(b, h->sync_stream, h->sync_pin, h->sms, tile, &h->pool);
     if (s == PLP_OK) {
         std::lock_guard<std::mutex> lk(h->mu);
         remember_tile(h->tile, tile);
@@ -1735,7 +1779,7 @@ int plp_batch_fetch(plp_batch* pb, plp_result** results) {
     std::lock_guard<std::mutex> g(h->sync_mu);
     cudaSetDevice(h->device);
     const double t0 = now_seconds();
-    int s = batch_fetch(pb->b, h->sync_stream);
+    int s = batch_fetch(pb->b, h->sync_stream, nullptr, &h->pool);
     if (s != PLP_OK) {
         record(h, s);
         return s;

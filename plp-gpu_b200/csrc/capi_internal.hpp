@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -19,19 +20,41 @@ struct plp_instance {
 // packed form (8 bytes each) and expanded on request.
 struct plp_result {
     int restarts = 0;
+    // plain path: summaries and expanded rows
     std::vector<plp_summary> summ;
-    // plain path: expanded rows
     std::vector<plpb::Placement> rows;
     std::vector<long long> row_off;           // restarts + 1 (plain path)
-    // device path: packed words, `stride` per restart (or per kept restart)
-    std::vector<unsigned long long> packed;
-    std::vector<int> packed_slot;             // restart -> index into packed (-1: not kept)
+    // device path: the decoders' slot heads and packed placement words,
+    // read in place from a host block shared by the results of one batch
+    std::shared_ptr<const char> block;
+    const plpb::SlotHead* heads = nullptr;    // one per restart
+    const unsigned long long* packed = nullptr;   // `stride` words per kept restart
+    bool kept_all = true;                     // false: only the best restart's placements
+    long long seed0 = 0;                      // seed of restart 0
+    double time_s = 0;
     int stride = 0;
     std::vector<plpb::TypeOrs> ors;
     int L = 0, W = 0, H = 0;
     std::vector<int> steps;                   // type of each decode step
     int best = -1;
     int best_fallback = 1;
+
+    plp_summary summary(int k) const {
+        if (!heads) return summ[k];
+        const plpb::SlotHead& h = heads[k];
+        plp_summary s;
+        s.n_boxes = h.n_boxes;
+        s.fallback = h.fallback;
+        s.volume = h.volume;
+        s.score = h.score;
+        s.n_passes = h.n_passes;
+        s.err = h.err;
+        s.seed = seed0 + k;
+        s.time_s = time_s;
+        return s;
+    }
+    // index of restart k's placements in `packed` (-1: not kept)
+    int packed_slot(int k) const { return kept_all ? k : (k == best ? 0 : -1); }
 };
 
 namespace plpb {
