@@ -185,8 +185,11 @@ int plp_set_tile(plp_handle* h, int32_t P, int32_t C, int32_t G, int32_t D, int3
 /* Autotuner (no reference counterpart): times candidate tiles -- one warp per
  * decoder with placed-box depth P, live-point depth C, decoders per CTA D and
  * minimum CTAs per SM M -- on a strided sample of at most max_decodes of the
- * workload's decodes (0 = 8192), each after a warm-up run, and keeps the
- * fastest as the handle's tile. tile_out (may be NULL) receives {P, C, G, D, M}.
+ * workload's decodes (0 = 32768), each after a warm-up run, and keeps the
+ * fastest as the handle's tile. A candidate's estimate scales the sample's
+ * decoder launch to the whole workload and adds the retry stage (restarts that
+ * outgrew the tile, re-run at a deeper one) at its latency, which does not
+ * shrink with the sample. tile_out (may be NULL) receives {P, C, G, D, M}.
  * The tile never changes results. */
 int plp_autotune(plp_handle* h, const plp_instance* const* insts, int32_t n_inst,
                  const plp_run_opts* opts, int32_t n_opts, int32_t max_decodes, int32_t* tile_out);

@@ -41,6 +41,7 @@ struct BlockArgs {
     const int* __restrict__ tab;
     const int2* __restrict__ work;
     int n_work;
+    const int* n_work_dev;         // set: the work count, written by an earlier launch
     int* work_next;
     int* err_flag;
     int* abort;
@@ -347,12 +348,13 @@ __device__ __forceinline__ void block_body(const BlockArgs& a, unsigned char* ba
     unsigned short* zt = a.Hz ? reinterpret_cast<unsigned short*>(base + lay.off_zt) : nullptr;
     unsigned char* fsr_base = base + lay.off_key;
 
+    const int n_work = a.n_work_dev ? *a.n_work_dev : a.n_work;
     for (;;) {
         if (*reinterpret_cast<volatile int*>(a.abort)) return;
         int item = 0;
         if (lane == 0) item = atomicAdd(a.work_next, 1);
         item = __shfl_sync(FULL, item, 0);
-        if (item >= a.n_work) break;
+        if (item >= n_work) break;
         const int2 wk = a.work[item];
         const InstDesc I = a.inst[wk.x];
         const int restart = wk.y;
@@ -639,15 +641,13 @@ cudaError_t block_occupancy(int P, int C, int N, int T, int Hz, int D, int M, in
     BlockFn fn = block_fn(D, M);
     if (!fn) return cudaErrorInvalidConfiguration;
     const int smem = block_smem_bytes(P, C, N, T, Hz) * D;
-    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    if (e != cudaSuccess) return e;
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas_per_sm, fn, 32 * D, smem);
+    return cached_occupancy(reinterpret_cast<const void*>(fn), 32 * D, smem, ctas_per_sm);
 }
 
 cudaError_t configure_block(const DecodeLaunch& L) {
     BlockFn fn = block_fn(L.decoders_per_cta, L.min_blocks);
     if (!fn) return cudaErrorInvalidConfiguration;
-    return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, block_launch_smem(L));
+    return ensure_dyn_smem(reinterpret_cast<const void*>(fn), block_launch_smem(L));
 }
 
 cudaError_t enqueue_block(const DecodeLaunch& L, cudaStream_t st) {
@@ -664,6 +664,7 @@ cudaError_t enqueue_block(const DecodeLaunch& L, cudaStream_t st) {
     a.tab = L.btab;
     a.work = L.work;
     a.n_work = L.n_work;
+    a.n_work_dev = L.n_work_dev;
     a.work_next = L.work_next;
     a.err_flag = L.err_flag;
     a.abort = L.abort;

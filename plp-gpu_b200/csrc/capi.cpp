@@ -267,6 +267,8 @@ struct Batch {
     cudaGraphExec_t gexec = nullptr;
     TileConfig gtile;
     int glaunches = 0;
+    bool gstaged = false;                  // the graph holds the device retry stage
+    size_t stage_slots = 0;                // work size that decides the retry stage (0: this batch's)
     // host results: one block of [slot heads | best per instance | packed
     // placements (all slots, or the gathered best per instance)], shared
     // with the result objects that read it in place
@@ -403,7 +405,9 @@ struct Batch {
         o_bcat = o;    o = al(o + std::max<size_t>(1, bcat.size()) * sizeof(BlkShape));
         o_btab = o;    o = al(o + std::max<size_t>(1, btab.size()) * sizeof(int));
         o_work = o;    o = al(o + work.size() * sizeof(int2));
-        o_next = o;    o = al(o + 16);
+        // counters and flags: [0] work counter, [4] retry-stage work counter,
+        // [8] error flag, [12] abort, [16] retry-stage error flag, [20] retry count
+        o_next = o;    o = al(o + 32);
         o_heads = o;   o = al(o + n_slots * sizeof(SlotHead));
         o_places = o;  o = al(o + std::max<long long>(1, n_places) * 8);
         o_best = o;    o = al(o + desc.size() * sizeof(int2));
@@ -565,6 +569,8 @@ namespace {
 struct ExecStats {
     double device_ms = 0, decoder_ms = 0;
     int launches = 0;
+    int redo = 0;                 // restarts the device retry stage ran again
+    long long redo_wave = 0;      // resident decoders of the retry stage's tile
 };
 
 int batch_release(Batch& b, cudaStream_t st) {
@@ -701,32 +707,113 @@ cudaError_t enqueue_select(Batch& b, cudaStream_t st, int* launches) {
     return cudaSuccess;
 }
 
+constexpr int FATAL_BITS = (1 << ERR_RNG) | (1 << ERR_SYNC);
+
+// The device retry stage. In a batch whose restarts take more than one wave of
+// resident decoders, a tile deep enough for the largest restart costs every
+// restart occupancy. Such a batch instead runs at its tile and, in the same
+// stream pass, runs the restarts that overflowed it again at a deeper tile
+// (P and C doubled) over a list the device builds. Returns whether the stage
+// applies and its tile.
+bool redo_stage(const Batch& b, const TileConfig& t, int sms, TileConfig* deep, long long* deep_wave = nullptr) {
+    int occ = 1;
+    if (tile_occupancy(b, t, &occ) != cudaSuccess || occ < 1) {
+        cudaGetLastError();
+        return false;
+    }
+    const size_t slots = b.stage_slots ? b.stage_slots : b.work.size();
+    if ((long long)slots <= (long long)sms * occ * t.D) return false;   // one wave
+    TileConfig d = t;
+    d.P = std::min(P_MAX, t.P * 2);
+    d.C = std::min(C_MAX, t.C * 2);
+    if (d.P == t.P && d.C == t.C) return false;
+    while (d.D > 1 && tile_smem(b, d) * d.D > 200 * 1024) d.D >>= 1;
+    fit_tile(d, b);
+    if (tile_smem(b, d) > 227 * 1024 || !tile_supported(b, d)) return false;
+    if (deep_wave) {
+        int occ2 = 1;
+        if (tile_occupancy(b, d, &occ2) != cudaSuccess || occ2 < 1) {
+            cudaGetLastError();
+            occ2 = 1;
+        }
+        *deep_wave = (long long)sms * occ2 * d.D;
+    }
+    *deep = d;
+    return true;
+}
+
+// the retry stage's decoder launch: the device-built list, its own work
+// counter and error flag, the count read at kernel start
+DecodeLaunch redo_launch(const Batch& b, const TileConfig& deep, int sms) {
+    DecodeLaunch L = make_launch(b, deep, reinterpret_cast<const int2*>(b.d_mem + b.o_redo), (int)b.work.size(), sms);
+    L.n_work_dev = reinterpret_cast<const int*>(b.d_mem + b.o_next + 20);
+    L.work_next = reinterpret_cast<int*>(b.d_mem + b.o_next + 4);
+    L.err_flag = reinterpret_cast<int*>(b.d_mem + b.o_next + 16);
+    return L;
+}
+
+// stream operations of the retry stage (capturable): list, then decoder
+cudaError_t enqueue_redo(Batch& b, const DecodeLaunch& L, int sms, cudaStream_t st, int* launches) {
+    cudaError_t e = launch_redo_collect(reinterpret_cast<const int2*>(b.d_mem + b.o_work), (int)b.work.size(),
+                                        reinterpret_cast<const InstDesc*>(b.d_mem + b.o_desc),
+                                        reinterpret_cast<const SlotHead*>(b.d_mem + b.o_heads),
+                                        reinterpret_cast<int2*>(b.d_mem + b.o_redo),
+                                        reinterpret_cast<int*>(b.d_mem + b.o_next + 20), sms, st);
+    if (e != cudaSuccess) return e;
+    (*launches)++;
+    e = enqueue_decoder(L, st);
+    if (e != cudaSuccess) return e;
+    (*launches)++;
+    return cudaSuccess;
+}
+
+// Flags of an execution, as copied to the pinned words [flag, abort, retry
+// flag, retry count]: the bits still to handle on the host -- fatal bits of
+// either launch, and capacity bits of the last launch that ran each restart.
+int pending_bits(const Batch& b, bool staged) {
+    const volatile int* fl = reinterpret_cast<const volatile int*>(b.h_flag);
+    return staged ? (fl[2] | (fl[0] & FATAL_BITS)) : fl[0];
+}
+
 // Records a clean execution of the batch with tile t as one CUDA graph:
-// error-flag reset, the persistent decoder, the flag copy to the pinned word,
-// selection and gather, with event ev[1] between decoder and selection. A
-// capture that fails leaves the batch on direct launches.
+// error-flag reset, the persistent decoder, the retry stage where it applies,
+// the flag copy to the pinned words, selection and gather, with event ev[1]
+// after the first decoder. A capture that fails leaves the batch on direct
+// launches.
 void batch_capture(Batch& b, cudaStream_t st, int sms, const TileConfig& t) {
     if (b.gexec) {
         cudaGraphExecDestroy(b.gexec);
         b.gexec = nullptr;
     }
+    // launch shapes and function attributes: before capture
     const DecodeLaunch L = make_launch(b, t, reinterpret_cast<const int2*>(b.d_mem + b.o_work),
-                                       (int)b.work.size(), sms);   // occupancy query: before capture
+                                       (int)b.work.size(), sms);
     if (configure_decoder(L) != cudaSuccess) {
         cudaGetLastError();
         return;
     }
-    int* d_flag = reinterpret_cast<int*>(b.d_mem + b.o_next + 8);
+    TileConfig deep;
+    const bool staged = redo_stage(b, t, sms, &deep);
+    DecodeLaunch L2{};
+    if (staged) {
+        L2 = redo_launch(b, deep, sms);
+        if (configure_decoder(L2) != cudaSuccess) {
+            cudaGetLastError();
+            return;
+        }
+    }
+    char* d_flag = b.d_mem + b.o_next + 8;
     if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
         cudaGetLastError();
         return;
     }
     int n = 0;
-    cudaError_t e = cudaMemsetAsync(d_flag, 0, 8, st);
+    cudaError_t e = cudaMemsetAsync(d_flag, 0, 16, st);
     if (e == cudaSuccess) e = enqueue_decoder(L, st);
     if (e == cudaSuccess) n++;
     if (e == cudaSuccess) e = cudaEventRecord(b.ev[1], st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(b.h_flag, d_flag, 4, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess && staged) e = enqueue_redo(b, L2, sms, st, &n);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(b.h_flag, d_flag, 16, cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = enqueue_select(b, st, &n);
     cudaGraph_t g = nullptr;
     const cudaError_t e2 = cudaStreamEndCapture(st, &g);
@@ -736,15 +823,17 @@ void batch_capture(Batch& b, cudaStream_t st, int sms, const TileConfig& t) {
             b.gexec = x;
             b.gtile = t;
             b.glaunches = n;
+            b.gstaged = staged;
         }
     }
     if (g) cudaGraphDestroy(g);
     cudaGetLastError();
 }
 
-// tile: in = tile to use, out = tile that succeeded (deeper after retries).
-// graph: capture a clean execution and replay it on later calls (batches
-// that run more than once).
+// tile: in = tile to use, out = tile to start the next execution with (deeper
+// after host retries of a one-wave batch, or when the retry stage ran more
+// than a quarter of the restarts). graph: capture a clean execution and
+// replay it on later calls (batches that run more than once).
 int batch_execute(Batch& b, cudaStream_t st, int sms, TileConfig& tile, ExecStats* xs, bool graph) {
     auto fail = [&](const char* what, cudaError_t err) {
         const int s = set_cuda_error(what, err);
@@ -753,6 +842,7 @@ int batch_execute(Batch& b, cudaStream_t st, int sms, TileConfig& tile, ExecStat
         set_error(s, keep);
         return s;
     };
+    const volatile int* fl = reinterpret_cast<const volatile int*>(b.h_flag);
     ExecStats x;
     TileConfig t = tile;
     fit_tile(t, b);
@@ -763,7 +853,7 @@ int batch_execute(Batch& b, cudaStream_t st, int sms, TileConfig& tile, ExecStat
         if (e == cudaSuccess) e = cudaEventRecord(b.ev[2], st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
         if (e != cudaSuccess) return fail("graph execution", e);
-        if (*reinterpret_cast<volatile int*>(b.h_flag) == 0) {
+        if (pending_bits(b, b.gstaged) == 0) {
             float ms = 0, dms = 0;
             cudaEventElapsedTime(&ms, b.ev[0], b.ev[2]);
             if (cudaEventElapsedTime(&dms, b.ev[0], b.ev[1]) != cudaSuccess) {
@@ -777,21 +867,29 @@ int batch_execute(Batch& b, cudaStream_t st, int sms, TileConfig& tile, ExecStat
             if (xs) *xs = x;
             return PLP_OK;
         }
-        // an error flag: run again on direct launches, which handle it
+        // flags left to handle: run again on direct launches, which handle them
     }
     const int2* d_work = reinterpret_cast<const int2*>(b.d_mem + b.o_work);
-    int* d_flag = reinterpret_cast<int*>(b.d_mem + b.o_next + 8);
-    // decoder, error-flag copy and selection in one stream pass with a single
-    // synchronisation; a raised flag (rare) re-runs the affected restarts
-    // below and selects again
-    cudaError_t e = cudaMemsetAsync(d_flag, 0, 8, st);
+    char* d_flag = b.d_mem + b.o_next + 8;
+    // decoder, retry stage, flag copy and selection in one stream pass with a
+    // single synchronisation; flags left over (rare) re-run the affected
+    // restarts below and select again
+    TileConfig deep;
+    const bool staged = redo_stage(b, t, sms, &deep, &x.redo_wave);
+    cudaError_t e = cudaMemsetAsync(d_flag, 0, 16, st);
     if (e != cudaSuccess) return fail("flag reset", e);
     e = cudaEventRecord(b.ev[0], st);
     if (e == cudaSuccess) e = launch_decoder(make_launch(b, t, d_work, (int)b.work.size(), sms), st);
     if (e == cudaSuccess) e = cudaEventRecord(b.ev[1], st);
     if (e != cudaSuccess) return fail("decoder launch", e);
     x.launches++;
-    e = cudaMemcpyAsync(b.h_flag, d_flag, 4, cudaMemcpyDeviceToHost, st);
+    if (staged) {
+        const DecodeLaunch L2 = redo_launch(b, deep, sms);
+        e = configure_decoder(L2);
+        if (e == cudaSuccess) e = enqueue_redo(b, L2, sms, st, &x.launches);
+        if (e != cudaSuccess) return fail("retry stage launch", e);
+    }
+    e = cudaMemcpyAsync(b.h_flag, d_flag, 16, cudaMemcpyDeviceToHost, st);
     if (e != cudaSuccess) return fail("flag copy", e);
     {
         int n = 0;
@@ -805,16 +903,20 @@ int batch_execute(Batch& b, cudaStream_t st, int sms, TileConfig& tile, ExecStat
     float ms = 0;
     cudaEventElapsedTime(&ms, b.ev[0], b.ev[1]);
     x.decoder_ms = ms;
-    // capacity retries: restarts whose live points or boxes outgrew the tile
-    // run again with a deeper tile (same slots, so results land in place)
+    const int staged_count = staged ? fl[3] : 0;
+    x.redo = staged_count;
+    // host retries: restarts whose live points or boxes outgrew the last
+    // tile they ran with run again with a deeper one (same slots, so results
+    // land in place)
+    TileConfig tr = staged ? deep : t;
     bool retried = false;
-    for (int attempt = 0; *reinterpret_cast<volatile int*>(b.h_flag) != 0; attempt++) {
+    for (int attempt = 0, bits = pending_bits(b, staged); bits != 0; attempt++, bits = fl[0]) {
         retried = true;
-        if (*reinterpret_cast<volatile int*>(b.h_flag) & (1 << ERR_RNG)) {
+        if (bits & (1 << ERR_RNG)) {
             batch_release(b, st);
             return set_error(PLP_E_DEVICE, "decoder reported an RNG rejection-bound error");
         }
-        if (*reinterpret_cast<volatile int*>(b.h_flag) & (1 << ERR_SYNC)) {
+        if (bits & (1 << ERR_SYNC)) {
             batch_release(b, st);
             return set_error(PLP_E_DEVICE, "decoder warps stopped meeting at a barrier (bounded wait gave up)");
         }
@@ -834,12 +936,12 @@ int batch_execute(Batch& b, cudaStream_t st, int sms, TileConfig& tile, ExecStat
             batch_release(b, st);
             return set_error(PLP_E_CAPACITY, "decoder tile capacity exceeded after retries");
         }
-        if (grow_p) t.P = std::min(P_MAX, std::max(t.P * 2, 32));
-        if (grow_c) t.C = std::min(C_MAX, t.C * 2);
+        if (grow_p) tr.P = std::min(P_MAX, std::max(tr.P * 2, 32));
+        if (grow_c) tr.C = std::min(C_MAX, tr.C * 2);
         // deeper tiles: fewer decoders per CTA keeps one CTA within 227 KB
-        while (t.D > 1 && tile_smem(b, t) * t.D > 200 * 1024) t.D >>= 1;
-        fit_tile(t, b);
-        if (tile_smem(b, t) > 227 * 1024 || !tile_supported(b, t)) {
+        while (tr.D > 1 && tile_smem(b, tr) * tr.D > 200 * 1024) tr.D >>= 1;
+        fit_tile(tr, b);
+        if (tile_smem(b, tr) > 227 * 1024 || !tile_supported(b, tr)) {
             batch_release(b, st);
             return set_error(PLP_E_CAPACITY, "instance needs a larger tile than shared memory holds");
         }
@@ -847,7 +949,7 @@ int batch_execute(Batch& b, cudaStream_t st, int sms, TileConfig& tile, ExecStat
         int2* d_redo = reinterpret_cast<int2*>(b.d_mem + b.o_redo);
         e = cudaMemcpyAsync(d_redo, b.redo_host.data(), redo.size() * sizeof(int2), cudaMemcpyHostToDevice, st);
         if (e == cudaSuccess) e = cudaMemsetAsync(d_flag, 0, 8, st);
-        if (e == cudaSuccess) e = launch_decoder(make_launch(b, t, d_redo, (int)redo.size(), sms), st);
+        if (e == cudaSuccess) e = launch_decoder(make_launch(b, tr, d_redo, (int)redo.size(), sms), st);
         if (e == cudaSuccess) e = cudaMemcpyAsync(b.h_flag, d_flag, 4, cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
         if (e != cudaSuccess) return fail("decoder relaunch", e);
@@ -865,16 +967,16 @@ int batch_execute(Batch& b, cudaStream_t st, int sms, TileConfig& tile, ExecStat
     cudaEventElapsedTime(&ms, b.ev[0], b.ev[2]);
     x.device_ms = ms;
     if (graph && !retried) batch_capture(b, st, sms, t);
-    tile = t;
+    if (staged) {
+        if ((long long)staged_count * 4 > (long long)b.work.size()) tile = deep;
+        else tile = t;
+    } else {
+        tile = tr;
+    }
     if (xs) *xs = x;
     return PLP_OK;
 }
 
-// Results that fit the thread's pinned staging buffer as it is come through
-// it (full-bandwidth copies, read in place by collect); others go straight to
-// pageable memory. The buffer is never grown for results: growing it frees
-// pinned memory, which synchronises the whole device and would stall every
-// other stream's work.
 // Copies a finished batch's results to the host. With a pool the copies land
 // in a pooled pinned block that the results keep; else in a pageable block,
 // staged through the thread's pinned buffer when it is large enough (the
@@ -994,6 +1096,7 @@ struct plp_handle {
     bool stop = false;
     int n_workers = 4;
     int busy_workers = 0;
+    int workers_ready = 0;
     std::vector<std::thread> workers;
     std::vector<cudaStream_t> streams;
     // synchronous solves
@@ -1024,6 +1127,14 @@ void worker_main(plp_handle* h, int wi) {
     cudaSetDevice(h->device);
     Pinned pin;
     cudaStream_t st = h->streams[wi];
+    // pinned flag word, events and a staging buffer for a typical request,
+    // made before the first request rather than inside its latency
+    if (pin.ensure_ctx() != cudaSuccess || pin.ensure((size_t)4 << 20) != cudaSuccess) cudaGetLastError();
+    {
+        std::lock_guard<std::mutex> lk(h->mu);
+        h->workers_ready++;
+    }
+    h->cv.notify_all();
     for (;;) {
         std::vector<Request*> wave;
         size_t wave_bytes = 0;
@@ -1390,6 +1501,10 @@ int plp_create(size_t budget_bytes, int32_t device, plp_handle** out) {
         if (e != cudaSuccess) return set_cuda_error("stream creation", e);
     }
     for (int i = 0; i < h->n_workers; i++) h->workers.emplace_back(worker_main, h, i);
+    {
+        std::unique_lock<std::mutex> lk(h->mu);
+        h->cv.wait_for(lk, std::chrono::seconds(10), [&] { return h->workers_ready == h->n_workers; });
+    }
     *out = h;
     return PLP_OK;
 }
@@ -1466,7 +1581,7 @@ int plp_autotune(plp_handle* h, const plp_instance* const* insts, int32_t n_inst
     }
     // strided sample of the longest-first work list keeps its mix of lengths
     const size_t n = full.work.size();
-    const size_t m = std::min(n, (size_t)(max_decodes ? max_decodes : 8192));
+    const size_t m = std::min(n, (size_t)(max_decodes ? max_decodes : 32768));
     std::vector<int2> sample(m);
     for (size_t k = 0; k < m; k++) sample[k] = full.work[k * n / m];
     // candidate tiles: one warp per decoder; depths around the instance sizes
@@ -1476,7 +1591,7 @@ int plp_autotune(plp_handle* h, const plp_instance* const* insts, int32_t n_inst
     for (int p : {64, 128, 256})
         if (p <= P_MAX && (p >= std::min(max_steps, 64) || p == 128)) Ps.push_back(p);
     for (int c : {256, 384, 512, 768}) Cs.push_back(c);
-    const int dm[][2] = {{8, 1}, {8, 2}, {4, 1}, {4, 4}, {2, 1}};
+    const int dm[][2] = {{1, 1}, {2, 1}, {4, 1}, {8, 1}, {8, 2}};
     std::vector<TileConfig> cand;
     for (int p : Ps)
         for (int c : Cs)
@@ -1495,11 +1610,18 @@ int plp_autotune(plp_handle* h, const plp_instance* const* insts, int32_t n_inst
         std::lock_guard<std::mutex> lk(h->mu);
         best = h->tile;
     }
+    // The estimate for the whole workload scales the sample's first decoder
+    // launch by n / m. What follows it (the retry stage, selection) is mostly
+    // the latency of the longest re-run restart, the same for the whole
+    // workload as for the sample, so it is added once, or once per wave of the
+    // retry tile that the scaled re-run count fills.
+    const double scale = (double)n / (double)std::max<size_t>(m, 1);
     for (const TileConfig& t0 : cand) {
         Batch b;
         s = b.build(in, op);
         if (s != PLP_OK) break;
         b.work = sample;
+        b.stage_slots = n;   // the retry stage as the whole workload would run it
         TileConfig t = t0;
         s = batch_prepare(b, h->sync_stream, h->sync_pin, h->sms, t, true);
         if (s != PLP_OK) break;
@@ -1508,7 +1630,10 @@ int plp_autotune(plp_handle* h, const plp_instance* const* insts, int32_t n_inst
             ExecStats x;
             TileConfig u = t0;
             s = batch_execute(b, h->sync_stream, h->sms, u, &x, false);
-            if (s == PLP_OK && rep > 0) ms = std::min(ms, x.device_ms);
+            if (s == PLP_OK && rep > 0) {
+                const double waves = x.redo_wave > 0 ? std::max(1.0, x.redo * scale / (double)x.redo_wave) : 1.0;
+                ms = std::min(ms, x.decoder_ms * scale + (x.device_ms - x.decoder_ms) * waves);
+            }
         }
         if (s != PLP_OK) break;   // batch_execute released the batch
         batch_release(b, h->sync_stream);

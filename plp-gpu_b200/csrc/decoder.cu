@@ -53,6 +53,9 @@
 #include <climits>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <type_traits>
 #include <vector>
 
@@ -154,6 +157,7 @@ struct DecoderArgs {
     const TypeOrs* __restrict__ types;
     const int2* __restrict__ work;
     int n_work;
+    const int* n_work_dev;         // set: the work count, written by an earlier launch
     int* work_next;
     int* err_flag;
     int* abort;
@@ -550,13 +554,14 @@ __device__ __forceinline__ void decoder_body(const DecoderArgs& a, unsigned char
         return;                           \
     }
 
+    const int n_work = a.n_work_dev ? *a.n_work_dev : a.n_work;
     for (;;) {
         if (*reinterpret_cast<volatile int*>(a.abort)) return;
         if (g == 0 && lane == 0) sh->item = atomicAdd(a.work_next, 1);
         PLP_SYNC()
         const int item = sh->item;
         PLP_SYNC()   // everyone has the item before it can change
-        if (item >= a.n_work) break;
+        if (item >= n_work) break;
         const int2 wk = a.work[item];
         const InstDesc I = a.inst[wk.x];
         const int restart = wk.y;
@@ -1180,12 +1185,13 @@ __device__ __forceinline__ void decoder1_body(const DecoderArgs& a, unsigned cha
     unsigned short* wi = reinterpret_cast<unsigned short*>(base + lay.off_wi);
     unsigned short* zt = a.Hz ? reinterpret_cast<unsigned short*>(base + lay.off_zt) : nullptr;
 
+    const int n_work = a.n_work_dev ? *a.n_work_dev : a.n_work;
     for (;;) {
         if (*reinterpret_cast<volatile int*>(a.abort)) return;
         int item = 0;
         if (lane == 0) item = atomicAdd(a.work_next, 1);
         item = __shfl_sync(FULL, item, 0);
-        if (item >= a.n_work) break;
+        if (item >= n_work) break;
         const int2 wk = a.work[item];
         const InstDesc I = a.inst[wk.x];
         const int restart = wk.y;
@@ -1576,6 +1582,45 @@ static DecoderFn decoder_fn(int G, int D, int M, int sup16 = 0) {
 
 bool decoder_config_supported(int G, int D, int M) { return decoder_fn(G, D, M) != nullptr; }
 
+namespace {
+std::mutex g_attr_mu;
+std::map<std::pair<const void*, int>, int> g_dyn_smem;                 // (kernel, device) -> limit set
+std::map<std::tuple<const void*, int, int, int>, int> g_occupancy;    // (kernel, device, threads, smem)
+}  // namespace
+
+cudaError_t ensure_dyn_smem(const void* fn, int smem) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lk(g_attr_mu);
+    int& cur = g_dyn_smem[{fn, dev}];
+    if (smem <= cur) return cudaSuccess;
+    e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e == cudaSuccess) cur = smem;
+    return e;
+}
+
+cudaError_t cached_occupancy(const void* fn, int threads, int smem, int* ctas_per_sm) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    {
+        std::lock_guard<std::mutex> lk(g_attr_mu);
+        auto it = g_occupancy.find(std::make_tuple(fn, dev, threads, smem));
+        if (it != g_occupancy.end()) {
+            *ctas_per_sm = it->second;
+            return cudaSuccess;
+        }
+    }
+    e = ensure_dyn_smem(fn, smem);
+    if (e != cudaSuccess) return e;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas_per_sm, fn, threads, (size_t)smem);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lk(g_attr_mu);
+    g_occupancy[std::make_tuple(fn, dev, threads, smem)] = *ctas_per_sm;
+    return cudaSuccess;
+}
+
 static DecoderArgs decoder_args(const DecodeLaunch& L) {
     DecoderArgs a;
     a.inst = L.inst;
@@ -1583,6 +1628,7 @@ static DecoderArgs decoder_args(const DecodeLaunch& L) {
     a.types = L.types;
     a.work = L.work;
     a.n_work = L.n_work;
+    a.n_work_dev = L.n_work_dev;
     a.work_next = L.work_next;
     a.err_flag = L.err_flag;
     a.abort = L.abort;
@@ -1606,7 +1652,7 @@ cudaError_t configure_decoder(const DecodeLaunch& L) {
     if (L.engine == 1) return configure_block(L);
     DecoderFn fn = decoder_fn(L.warps_per_decoder, L.decoders_per_cta, L.min_blocks, L.sup16);
     if (!fn) return cudaErrorInvalidConfiguration;
-    return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, decoder_launch_smem(L));
+    return ensure_dyn_smem(reinterpret_cast<const void*>(fn), decoder_launch_smem(L));
 }
 
 // Stream operations only (counter resets and the launch): capturable.
@@ -1632,9 +1678,27 @@ cudaError_t decoder_occupancy(int P, int C, int Hz, int G, int D, int M, int* ct
     DecoderFn fn = decoder_fn(G, D, M, sup16);
     if (!fn) return cudaErrorInvalidConfiguration;
     const int smem = decoder_smem_bytes(P, C, Hz, G, sup16) * D;
-    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    if (e != cudaSuccess) return e;
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas_per_sm, fn, 32 * G * D, smem);
+    return cached_occupancy(reinterpret_cast<const void*>(fn), 32 * G * D, smem, ctas_per_sm);
+}
+
+// Appends the work items whose restart overflowed its tile (box or live-point
+// capacity) to `redo`; `count` is zero on entry. The list's order does not
+// matter: each restart's results land in its own slot.
+__global__ void redo_collect_kernel(const int2* __restrict__ work, int n_work, const InstDesc* __restrict__ inst,
+                                    const SlotHead* __restrict__ heads, int2* __restrict__ redo,
+                                    int* __restrict__ count) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_work; i += gridDim.x * blockDim.x) {
+        const int2 w = work[i];
+        const int err = heads[inst[w.x].slot_base + w.y].err;
+        if (err == ERR_BOX_CAP || err == ERR_CAND_CAP) redo[atomicAdd(count, 1)] = w;
+    }
+}
+
+cudaError_t launch_redo_collect(const int2* work, int n_work, const InstDesc* inst, const SlotHead* heads,
+                                int2* redo, int* count, int sms, cudaStream_t st) {
+    const int blocks = std::max(1, std::min((n_work + 255) / 256, sms * 8));
+    redo_collect_kernel<<<blocks, 256, 0, st>>>(work, n_work, inst, heads, redo, count);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_select_best(const InstDesc* inst, int n_inst, const SlotHead* heads, int2* best,
@@ -1661,7 +1725,7 @@ cudaError_t launch_fsr(const int* rows7, const int* offsets, int n_pack, int cap
                        double* out_score, double* out_fsr, cudaStream_t st) {
     const int wpb = 4;
     const int smem = fsr_smem_per_warp(cap) * wpb;
-    cudaError_t e = cudaFuncSetAttribute(fsr_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaError_t e = ensure_dyn_smem(reinterpret_cast<const void*>(fsr_kernel), smem);
     if (e != cudaSuccess) return e;
     fsr_kernel<<<(n_pack + wpb - 1) / wpb, 32 * wpb, smem, st>>>(rows7, offsets, n_pack, cap, mu,
                                                                  out_score, out_fsr);
@@ -1672,7 +1736,7 @@ cudaError_t launch_item_order(const long long* vols, const int* qty, const int* 
                               const int* n_types, const long long* step_off, int n_inst, int order,
                               int* out_types, int sort_cap, cudaStream_t st) {
     const int smem = 8 * sort_cap;
-    cudaError_t e = cudaFuncSetAttribute(item_order_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaError_t e = ensure_dyn_smem(reinterpret_cast<const void*>(item_order_kernel), smem);
     if (e != cudaSuccess) return e;
     item_order_kernel<<<n_inst, 256, smem, st>>>(vols, qty, type_off, n_types, step_off, order,
                                                  out_types, sort_cap);

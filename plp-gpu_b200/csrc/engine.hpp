@@ -13,6 +13,7 @@ struct DecodeLaunch {
     const TypeOrs* types;
     const int2* work;
     int n_work;
+    const int* n_work_dev;    // set: the work count is read here at kernel start (n_work bounds it)
     int* work_next;
     int* err_flag;            // OR of (1 << err) over restarts that failed
     int* abort;               // set when a bounded barrier wait gives up
@@ -45,6 +46,17 @@ bool block_config_supported(int D, int M);
 cudaError_t block_occupancy(int P, int C, int N, int T, int Hz, int D, int M, int* ctas_per_sm);
 cudaError_t configure_block(const DecodeLaunch& L);
 cudaError_t enqueue_block(const DecodeLaunch& L, cudaStream_t st);
+// Per-device caches of kernel launch attributes: the dynamic shared-memory
+// limit is raised only when a launch needs more than every earlier launch of
+// the kernel on the device, and occupancy is queried once per (kernel,
+// device, block size, shared memory). Both calls change or read per-kernel
+// driver state, and made per solve they cost more than a small solve's host side.
+cudaError_t ensure_dyn_smem(const void* fn, int smem);
+cudaError_t cached_occupancy(const void* fn, int threads, int smem, int* ctas_per_sm);
+
+// work items whose restart overflowed its tile, appended to redo (count zeroed by the caller)
+cudaError_t launch_redo_collect(const int2* work, int n_work, const InstDesc* inst, const SlotHead* heads,
+                                int2* redo, int* count, int sms, cudaStream_t st);
 cudaError_t launch_select_best(const InstDesc* inst, int n_inst, const SlotHead* heads, int2* best,
                                cudaStream_t st);
 cudaError_t launch_rng_dump(const long long* seeds, int n_seeds, int n_random, int n_bits,

@@ -221,6 +221,28 @@ def test_time_budget_pass_cap_binds():
     assert _jsons(r) == _jsons(f)
 
 
+def test_retry_stage_small_tile_matches_oracle():
+    """A multi-wave batch (6400 restarts) at a tile too small for its larger
+    restarts: the restarts that overflow run again on the device at a deeper
+    tile in the same stream pass (and on the host beyond that). Results match
+    the oracle on every run."""
+    texts = [i.to_thpack() for i in synth.batched_set(40, 36000)]
+    insts = [P.Instance.parse(t) for t in texts]
+    with P.Handle() as h:
+        h.set_tile(64, 128, 1, 1, 1)
+        b = h.prepare(insts, P.make_opts(seed=5, restarts=160))
+        runs = [b.run() for _ in range(3)]
+        res = b.fetch()
+        b.close()
+    # decoder, retry list, retry decoder and selection at least
+    assert runs[0][2] >= 4, runs
+    for n, (t, r) in enumerate(zip(texts, res)):
+        oi = O.OInstance(t)
+        for k in range(n % 11, 160, 37):
+            js, _, _ = O.run(oi, seed=5 + k)
+            assert O.strip_time(r.json(k)) == O.strip_time(js), (n, k)
+
+
 def test_multi_wave_batch_matches_oracle():
     """A batch larger than one wave of resident decoders (3000 restarts) runs
     with the contact areas in 16 bits; a stride sample against the oracle."""
