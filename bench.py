@@ -366,6 +366,7 @@ def main():
     # (the block engine has no reference work replay: its roofline reports time only)
     T = [r.work(k)[0] for r, k in slots[::stride]] if args.workload != "block" else [0]
     t_mean = sum(T) / len(T)
+    del slots, warm_results   # their pinned result block goes back to the handle's pool
     clocks = Clocks(local)
     barrier()
     clocks.start()

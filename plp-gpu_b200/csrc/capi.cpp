@@ -487,8 +487,8 @@ struct Pinned {
 // Pinned host blocks that the results of synchronous solves are read from in
 // place: the device writes each result byte once, into memory the result
 // objects keep. A block returns to the free list when the last result
-// viewing it is freed, and the pool pins at most `limit` bytes (a solve that
-// finds no room copies into pageable memory instead). Pinned memory is freed
+// viewing it is freed, and the pool pins at most a quarter of host memory (a
+// solve that finds no room copies into pageable memory instead). Pinned memory is freed
 // only when the pool is destroyed with its handle: freeing it synchronises
 // the device.
 struct HostPool {
@@ -499,7 +499,7 @@ struct HostPool {
     HostPool() {
         const long pages = sysconf(_SC_PHYS_PAGES), page = sysconf(_SC_PAGESIZE);
         const size_t phys = pages > 0 && page > 0 ? (size_t)pages * (size_t)page : ((size_t)16 << 30);
-        limit = std::min((size_t)8 << 30, phys / 4);
+        limit = phys / 4;
     }
     ~HostPool() {
         for (auto& f : free_list) cudaFreeHost(f.first);
