@@ -364,8 +364,16 @@ def main():
     slots = [(r, k) for r in warm_results for k in range(r.restarts)]
     stride = max(1, len(slots) // 512)
     # (the block engine has no reference work replay: its roofline reports time only)
-    T = [r.work(k)[0] for r, k in slots[::stride]] if args.workload != "block" else [0]
+    sample = slots[::stride]
+    work = [r.work(k) for r, k in sample] if args.workload != "block" else [(0, 0)]
+    T = [w[0] for w in work]
     t_mean = sum(T) / len(T)
+    placed = [r.summary(k).n_boxes for r, k in sample]
+    pairs = [w[1] for w in work]
+    dist = {"placed_per_decode": [min(placed), sum(placed) / len(placed), max(placed)],
+            "pairs_per_decode": [min(pairs), sum(pairs) / len(pairs), max(pairs)],
+            "sampled_decodes": len(sample)}
+    del sample
     del slots, warm_results   # their pinned result block goes back to the handle's pool
     clocks = Clocks(local)
     barrier()
@@ -466,6 +474,9 @@ def main():
             "data": "synthetic (seeded generator, 587x233x220 container)",
             "config": {"workload": desc, "instances": len(insts), "restarts": R,
                        "items_per_instance": [min(n_items), max(n_items)],
+                       "distributions": {**dist, "note": "min, mean, max over the sampled decodes; pairs = "
+                                                         "(extreme point, orientation) pairs the reference "
+                                                         "evaluates per decode"},
                        "parallelism": f"dp{world} (restarts sharded by rank)",
                        "l2": "flushed between timed steps (256 MiB write)",
                        "tile": dict(zip(("P", "C", "G", "D", "M"), tile)), "tile_source": "--tile" if args.tile else "plp_autotune",

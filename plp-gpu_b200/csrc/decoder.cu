@@ -1069,17 +1069,14 @@ __device__ __forceinline__ int place1(int t, int pp, bool full, uint32_t* mt, in
         int s0 = 0, s1 = 0, s2 = 0, s3 = 0, s4 = 0, s5 = 0;
         bool mv_sup = false;
         if (i < nc) {
+            // all of a point's words load at once (in bounds; used if it moves)
             key = keys[i];
+            s = st[i];
+            s0 = sup[i]; s1 = sup[C + i]; s2 = sup[2 * C + i];
+            s3 = sup[3 * C + i]; s4 = sup[4 * C + i]; s5 = sup[5 * C + i];
             const int x = (int)(key & xmask), y = (int)((key >> xb) & ymask), z = (int)(key >> xyb);
             keep = !(px <= x && x < px2 && py <= y && y < py2 && pz <= z && z < pz2);
-            if (keep) {
-                s = st[i];
-                mv_sup = (s & ST_VALID) && z > 0;
-                if (mv_sup) {
-                    s0 = sup[i]; s1 = sup[C + i]; s2 = sup[2 * C + i];
-                    s3 = sup[3 * C + i]; s4 = sup[4 * C + i]; s5 = sup[5 * C + i];
-                }
-            }
+            mv_sup = keep && (s & ST_VALID) && z > 0;
         }
         const unsigned bal = __ballot_sync(FULL, keep);
         __syncwarp();
@@ -1134,11 +1131,9 @@ __device__ __forceinline__ int place1(int t, int pp, bool full, uint32_t* mt, in
             if (in) {
                 key = keys[i];
                 s = st[i];
+                s0 = sup[i]; s1 = sup[C + i]; s2 = sup[2 * C + i];
+                s3 = sup[3 * C + i]; s4 = sup[4 * C + i]; s5 = sup[5 * C + i];
                 mv_sup = (s & ST_VALID) && (key >> xyb) > 0;
-                if (mv_sup) {
-                    s0 = sup[i]; s1 = sup[C + i]; s2 = sup[2 * C + i];
-                    s3 = sup[3 * C + i]; s4 = sup[4 * C + i]; s5 = sup[5 * C + i];
-                }
 #pragma unroll
                 for (int c = 0; c < 8; c++) off += ((newm >> c) & 1u) && ckk[c] < key;
             }
