@@ -196,7 +196,15 @@ int plp_autotune(plp_handle* h, const plp_instance* const* insts, int32_t n_inst
 
 /* Synchronous batched solve: every restart of every instance in one
  * persistent decoder launch (plus a FSR/selection launch), results copied to
- * the host. opts holds n_inst entries (or 1 entry shared by all). */
+ * the host. opts holds n_inst entries (or 1 entry shared by all). A batch
+ * whose restarts take more than one wave of resident decoders re-runs the
+ * restarts that outgrew the tile at a deeper tile in the same stream pass.
+ * The results of one call share a pinned host block from the handle's pool,
+ * which the device writes once and the results read in place. It returns to
+ * the pool when the last of them is freed, so results may outlive the
+ * handle. The pool pins at most a quarter of host memory, or the environment
+ * variable PLP_PINNED_POOL_MB (read at plp_create; 0 turns it off); beyond
+ * that results go to pageable memory. */
 int plp_solve(plp_handle* h, const plp_instance* const* insts, int32_t n_inst,
               const plp_run_opts* opts, int32_t n_opts, plp_result** results);
 
@@ -205,9 +213,10 @@ int plp_solve(plp_handle* h, const plp_instance* const* insts, int32_t n_inst,
  * it wants them. plp_batch_run is synchronous; device_ms is the CUDA-event
  * time of all device work of the run, decoder_ms that of the decoder kernel
  * alone, launches the number of kernels launched. A run that needed no
- * capacity retry is captured as one CUDA graph (error-flag reset, decoder,
- * flag copy, selection, gather) and later runs with the same tile replay it
- * with a single graph launch and a single synchronisation. */
+ * host-side capacity retry is captured as one CUDA graph (error-flag reset,
+ * decoder, the device retry stage where it applies, flag copy, selection,
+ * gather) and later runs with the same tile replay it with a single graph
+ * launch and a single synchronisation. */
 typedef struct plp_batch plp_batch;
 int plp_batch_prepare(plp_handle* h, const plp_instance* const* insts, int32_t n_inst,
                       const plp_run_opts* opts, int32_t n_opts, plp_batch** out);

@@ -10,6 +10,7 @@
 #include <chrono>
 #include <climits>
 #include <condition_variable>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <map>
@@ -487,8 +488,9 @@ struct Pinned {
 // Pinned host blocks that the results of synchronous solves are read from in
 // place: the device writes each result byte once, into memory the result
 // objects keep. A block returns to the free list when the last result
-// viewing it is freed, and the pool pins at most a quarter of host memory (a
-// solve that finds no room copies into pageable memory instead). Pinned memory is freed
+// viewing it is freed, and the pool pins at most a quarter of host memory, or
+// PLP_PINNED_POOL_MB (a solve that finds no room copies into pageable memory
+// instead). Pinned memory is freed
 // only when the pool is destroyed with its handle: freeing it synchronises
 // the device.
 struct HostPool {
@@ -500,6 +502,11 @@ struct HostPool {
         const long pages = sysconf(_SC_PHYS_PAGES), page = sysconf(_SC_PAGESIZE);
         const size_t phys = pages > 0 && page > 0 ? (size_t)pages * (size_t)page : ((size_t)16 << 30);
         limit = phys / 4;
+        if (const char* v = std::getenv("PLP_PINNED_POOL_MB")) {   // operator override, 0 = off
+            char* end = nullptr;
+            const unsigned long long mb = std::strtoull(v, &end, 10);
+            if (end != v) limit = (size_t)mb << 20;
+        }
     }
     ~HostPool() {
         for (auto& f : free_list) cudaFreeHost(f.first);
