@@ -837,11 +837,59 @@ void batch_capture(Batch& b, cudaStream_t st, int sms, const TileConfig& t) {
     cudaGetLastError();
 }
 
+// Host destination of a batch's results: [slot heads | best per instance |
+// packed placements (all slots, or the gathered best per instance)]. With a
+// pool, a pooled pinned block that the results keep; else a pageable block,
+// staged through the thread's pinned buffer when it is large enough (that
+// buffer is reused by the thread's next batch, so it is copied out).
+struct ResultCopy {
+    std::shared_ptr<char> blk;
+    char* dst = nullptr;
+    char* stage = nullptr;
+    size_t hb = 0, bb = 0, pb = 0;
+};
+
+int result_dst(const Batch& b, Pinned* pin, const std::shared_ptr<HostPool>* pool, ResultCopy& rc) {
+    rc.hb = b.n_slots * sizeof(SlotHead);
+    rc.bb = b.desc.size() * sizeof(int2);
+    rc.pb = b.best_only ? b.desc.size() * (size_t)b.max_stride * 8 : (size_t)b.n_places * 8;
+    const size_t total = rc.hb + rc.bb + rc.pb;
+    if (pool && *pool) rc.blk = pool_take(*pool, total);
+    if (!rc.blk) {
+        if (pin && pin->p && total <= pin->cap) rc.stage = pin->p;
+        rc.blk = std::shared_ptr<char>(new (std::nothrow) char[std::max<size_t>(total, 1)], std::default_delete<char[]>());
+        if (!rc.blk) return set_error(PLP_E_CAPACITY, "host memory for the results could not be allocated");
+    }
+    rc.dst = rc.stage ? rc.stage : rc.blk.get();
+    return PLP_OK;
+}
+
+cudaError_t result_enqueue(const Batch& b, const ResultCopy& rc, cudaStream_t st) {
+    cudaError_t e = cudaMemcpyAsync(rc.dst, b.d_mem + b.o_heads, rc.hb, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(rc.dst + rc.hb, b.d_mem + b.o_best, rc.bb, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess && rc.pb)
+        e = cudaMemcpyAsync(rc.dst + rc.hb + rc.bb, b.d_mem + (b.best_only ? b.o_gather : b.o_places), rc.pb,
+                            cudaMemcpyDeviceToHost, st);
+    return e;
+}
+
+// after the copies completed: the batch's results view the block
+void result_take(Batch& b, ResultCopy& rc) {
+    if (rc.stage) std::memcpy(rc.blk.get(), rc.stage, rc.hb + rc.bb + rc.pb);
+    b.host = std::move(rc.blk);
+    b.heads_ptr = reinterpret_cast<const SlotHead*>(b.host.get());
+    b.best_ptr = reinterpret_cast<const int2*>(b.host.get() + rc.hb);
+    b.places_ptr = reinterpret_cast<const unsigned long long*>(b.host.get() + rc.hb + rc.bb);
+}
+
 // tile: in = tile to use, out = tile to start the next execution with (deeper
 // after host retries of a one-wave batch, or when the retry stage ran more
 // than a quarter of the restarts). graph: capture a clean execution and
-// replay it on later calls (batches that run more than once).
-int batch_execute(Batch& b, cudaStream_t st, int sms, TileConfig& tile, ExecStats* xs, bool graph) {
+// replay it on later calls (batches that run more than once). rc: copy the
+// results there in the same stream pass, after the final selection, so one
+// synchronisation covers execution and result copy.
+int batch_execute(Batch& b, cudaStream_t st, int sms, TileConfig& tile, ExecStats* xs, bool graph,
+                  const ResultCopy* rc = nullptr) {
     auto fail = [&](const char* what, cudaError_t err) {
         const int s = set_cuda_error(what, err);
         std::string keep = plpb_last();
@@ -858,6 +906,7 @@ int batch_execute(Batch& b, cudaStream_t st, int sms, TileConfig& tile, ExecStat
         cudaError_t e = cudaEventRecord(b.ev[0], st);
         if (e == cudaSuccess) e = cudaGraphLaunch(b.gexec, st);
         if (e == cudaSuccess) e = cudaEventRecord(b.ev[2], st);
+        if (e == cudaSuccess && rc) e = result_enqueue(b, *rc, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
         if (e != cudaSuccess) return fail("graph execution", e);
         if (pending_bits(b, b.gstaged) == 0) {
@@ -905,6 +954,7 @@ int batch_execute(Batch& b, cudaStream_t st, int sms, TileConfig& tile, ExecStat
         if (e != cudaSuccess) return fail("select launch", e);
     }
     e = cudaEventRecord(b.ev[2], st);
+    if (e == cudaSuccess && rc) e = result_enqueue(b, *rc, st);   // valid unless host retries follow
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return fail("decoder", e);
     float ms = 0;
@@ -968,6 +1018,7 @@ int batch_execute(Batch& b, cudaStream_t st, int sms, TileConfig& tile, ExecStat
         x.launches += n;
         if (e != cudaSuccess) return fail("select launch", e);
         e = cudaEventRecord(b.ev[2], st);
+        if (e == cudaSuccess && rc) e = result_enqueue(b, *rc, st);   // again, after the retries
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
         if (e != cudaSuccess) return fail("select", e);
     }
@@ -984,44 +1035,26 @@ int batch_execute(Batch& b, cudaStream_t st, int sms, TileConfig& tile, ExecStat
     return PLP_OK;
 }
 
-// Copies a finished batch's results to the host. With a pool the copies land
-// in a pooled pinned block that the results keep; else in a pageable block,
-// staged through the thread's pinned buffer when it is large enough (the
-// staging buffer is reused by the thread's next batch, so it is copied out).
+// Copies a finished batch's results to the host (destination as result_dst).
 int batch_fetch(Batch& b, cudaStream_t st, Pinned* pin = nullptr, const std::shared_ptr<HostPool>* pool = nullptr) {
-    const size_t hb = b.n_slots * sizeof(SlotHead), bb = b.desc.size() * sizeof(int2);
-    const size_t pb = b.best_only ? b.desc.size() * (size_t)b.max_stride * 8 : (size_t)b.n_places * 8;
-    const size_t total = hb + bb + pb;
-    std::shared_ptr<char> blk;
-    if (pool && *pool) blk = pool_take(*pool, total);
-    char* stage = nullptr;
-    if (!blk) {
-        if (pin && pin->p && total <= pin->cap) stage = pin->p;
-        blk = std::shared_ptr<char>(new (std::nothrow) char[std::max<size_t>(total, 1)], std::default_delete<char[]>());
-        if (!blk) {
-            batch_release(b, st);
-            return set_error(PLP_E_CAPACITY, "host memory for the results could not be allocated");
-        }
-    }
-    char* dst = stage ? stage : blk.get();
-    cudaError_t e = cudaMemcpyAsync(dst, b.d_mem + b.o_heads, hb, cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(dst + hb, b.d_mem + b.o_best, bb, cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess && pb)
-        e = cudaMemcpyAsync(dst + hb + bb, b.d_mem + (b.best_only ? b.o_gather : b.o_places), pb,
-                            cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    if (e != cudaSuccess) {
-        const int s = set_cuda_error("result copy", e);
+    ResultCopy rc;
+    int s = result_dst(b, pin, pool, rc);
+    if (s != PLP_OK) {
         std::string keep = plpb_last();
         batch_release(b, st);
         set_error(s, keep);
         return s;
     }
-    if (stage) std::memcpy(blk.get(), stage, total);
-    b.host = std::move(blk);
-    b.heads_ptr = reinterpret_cast<const SlotHead*>(b.host.get());
-    b.best_ptr = reinterpret_cast<const int2*>(b.host.get() + hb);
-    b.places_ptr = reinterpret_cast<const unsigned long long*>(b.host.get() + hb + bb);
+    cudaError_t e = result_enqueue(b, rc, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+        s = set_cuda_error("result copy", e);
+        std::string keep = plpb_last();
+        batch_release(b, st);
+        set_error(s, keep);
+        return s;
+    }
+    result_take(b, rc);
     return PLP_OK;
 }
 
@@ -1037,10 +1070,17 @@ int run_batch(Batch& b, cudaStream_t st, Pinned& pin, int sms, TileConfig& tile,
               const std::shared_ptr<HostPool>* pool = nullptr) {
     int s = batch_prepare(b, st, pin, sms, tile, true);
     if (s != PLP_OK) return s;
-    s = batch_execute(b, st, sms, tile, nullptr, false);
+    ResultCopy rc;
+    s = result_dst(b, &pin, pool, rc);
+    if (s != PLP_OK) {
+        std::string keep = plpb_last();
+        batch_release(b, st);
+        set_error(s, keep);
+        return s;
+    }
+    s = batch_execute(b, st, sms, tile, nullptr, false, &rc);   // results copied in the same pass
     if (s != PLP_OK) return s;
-    s = batch_fetch(b, st, &pin, pool);
-    if (s != PLP_OK) return s;
+    result_take(b, rc);
     return batch_release(b, st);
 }
 
