@@ -63,6 +63,24 @@ def test_block_engine_tiny_tile_retries_keep_results():
     assert got == ref
 
 
+def test_block_engine_retry_stage_multi_wave_matches_oracle():
+    """6400 restarts at a tiny tile: more than one wave, so the restarts that
+    overflow re-run on the device at a deeper tile in the same pass."""
+    texts = [i.to_thpack() for i in synth.batched_set(40, 34100)]
+    insts = [P.Instance.parse(t) for t in texts]
+    with P.Handle() as h:
+        h.set_tile(P=16, C=64, G=1, D=1, M=1)
+        b = h.prepare(insts, _opts(2, restarts=160))
+        runs = [b.run() for _ in range(2)]
+        res = b.fetch()
+        b.close()
+    assert runs[0][2] >= 4, runs   # decoder, retry list, retry decoder, selection
+    for n, (t, r) in enumerate(zip(texts, res)):
+        oi = O.OInstance(t)
+        for k in range(n % 7, 160, 53):
+            assert O.strip_time(r.json(k)) == O.strip_time(O.run_block(oi, seed=2 + k)), (n, k)
+
+
 def test_block_engine_batch_rejects_mixed_engines(handle):
     inst = P.Instance.parse(synth.single_pass(1).to_thpack())
     with pytest.raises(P.PlpError):
