@@ -1329,7 +1329,7 @@ __device__ __forceinline__ void decoder1_body(const DecoderArgs& a, unsigned cha
             }
             if (err != ERR_NONE) break;
             const double score =
-                fsr_score_warp(bx, bzs, z2s, bis, nb, I.mu, reinterpret_cast<char*>(keys), lane, nullptr);
+                fsr_score_warp(bx, bzs, z2s, bis, nb, I.mu, reinterpret_cast<char*>(keys), lane, nullptr, zt);
             const bool acc = !I.has_theta || score >= I.theta;
             bool take;
             if (acc) take = !have_acc || vol > best_vol || (vol == best_vol && nb > best_n);

@@ -17,9 +17,11 @@ namespace plpb {
 // the supports j are updated in parallel (each j by one lane), so every
 // load[j] receives its additions in the reference order.
 // ---------------------------------------------------------------------------
+// zt (may be null): the top-z index zt[z] = number of boxes with top < z, so
+// the boxes with top exactly z are [zt[z], zt[z + 1]) without a search.
 static __device__ __noinline__ double fsr_score_warp(const int4* bx, const int* bz, const int* z2,
                                  const unsigned short* bi, int n, double mu, char* scratch,
-                                 int lane, double* fsr_out) {
+                                 int lane, double* fsr_out, const unsigned short* zt = nullptr) {
     if (n == 0) return 0.0;
     double* load = reinterpret_cast<double*>(scratch);               // by sorted position
     uint32_t* key = reinterpret_cast<uint32_t*>(scratch + 8 * n);    // sort keys
@@ -64,7 +66,8 @@ static __device__ __noinline__ double fsr_score_warp(const int4* bx, const int* 
         const int zb = bz[p];
         int t = 0;
         if (zb > 0) {
-            for (int j = lower_bound_top(z2, n, zb); j < n && z2[j] == zb; j++) {
+            const int j0 = zt ? (int)zt[zb] : lower_bound_top(z2, n, zb);
+            for (int j = j0; j < n && z2[j] == zb; j++) {
                 const int4 c = bx[j];
                 const int ox = min(b.z, c.z) - max(b.x, c.x);
                 if (ox <= 0) continue;
@@ -83,9 +86,15 @@ static __device__ __noinline__ double fsr_score_warp(const int4* bx, const int* 
         int qe = q;
         while (qe < n && (int)(0xffff - (key[qe] >> 16)) == zl) qe++;
         if (zl > 0) {
-            const int jlo = lower_bound_top(z2, n, zl);
-            int jhi = jlo;
-            while (jhi < n && z2[jhi] == zl) jhi++;
+            int jlo, jhi;
+            if (zt) {
+                jlo = zt[zl];
+                jhi = zt[zl + 1];
+            } else {
+                jlo = lower_bound_top(z2, n, zl);
+                jhi = jlo;
+                while (jhi < n && z2[jhi] == zl) jhi++;
+            }
             for (int jb = jlo; jb < jhi; jb += 32) {
                 const int j = jb + lane;
                 if (j < jhi) {
