@@ -294,6 +294,24 @@ struct Batch {
         n_slots = 0; n_places = 0; max_stride = 1; max_steps = 0; multi_pass = false;
         int maxH = 0;
         best_only = true;
+        // item sequences of a large batch are sorted on several threads; the
+        // rest of the build is appends in instance order
+        std::vector<std::vector<int>> seqs;
+        if (in.size() >= 256) {
+            seqs.resize(in.size());
+            const unsigned hw = std::thread::hardware_concurrency();
+            const int nt = (int)std::max(1u, std::min(16u, hw ? hw : 1u));
+            std::atomic<size_t> next{0};
+            auto job = [&] {
+                for (size_t i0; (i0 = next.fetch_add(64)) < in.size();)
+                    for (size_t k = i0; k < std::min(in.size(), i0 + 64); k++)
+                        if (op[k].order == 0 || op[k].order == 1) seqs[k] = item_sequence(*in[k], op[k].order);
+            };
+            std::vector<std::thread> pool;
+            for (int t = 1; t < nt; t++) pool.emplace_back(job);
+            job();
+            for (auto& th : pool) th.join();
+        }
         for (size_t i = 0; i < in.size(); i++) {
             const Instance& I = *in[i];
             const plp_run_opts& o = op[i];
@@ -318,7 +336,7 @@ struct Batch {
                                  "must sum to <= 32)");
             if ((int)I.types.size() >= 8192)
                 return set_error(PLP_E_CAPACITY, "more than 8191 box types");
-            const std::vector<int> seq = item_sequence(I, o.order);
+            const std::vector<int> seq = seqs.empty() ? item_sequence(I, o.order) : std::move(seqs[i]);
             InstDesc d{};
             d.L = I.L; d.W = I.W; d.H = I.H;
             d.n_steps = (int)seq.size();

@@ -68,3 +68,19 @@ def test_batch_fetch_results_survive_rerun_and_close():
     oi = O.OInstance(texts[0])
     js, _, _ = O.run(oi, seed=1 + 5)
     assert before[0][5] == O.strip_time(js)
+
+
+def test_large_batch_build_matches_oracle():
+    """300 instances take the threaded item-sequence build; per-instance
+    options (volume or input order) stay with their instance."""
+    texts = [i.to_thpack() for i in synth.batched_set(300, 38000)]
+    insts = [P.Instance.parse(t) for t in texts]
+    orders = ["volume" if n % 3 else "input" for n in range(300)]
+    opts = [P.make_opts(seed=n, restarts=2, order=orders[n]) for n in range(300)]
+    with P.Handle() as h:
+        res = h.solve(insts, opts)
+    for n in range(0, 300, 13):
+        oi = O.OInstance(texts[n])
+        for k in range(2):
+            js, _, _ = O.run(oi, seed=n + k, order=orders[n])
+            assert O.strip_time(res[n].json(k)) == O.strip_time(js), (n, k)
