@@ -1099,10 +1099,25 @@ __device__ __forceinline__ int place1(int t, int pp, bool full, uint32_t* mt, in
     uint32_t ck = 0;
     int rank = 0;
     bool isnew = false;
-    if (lane < 8 && !((cov >> lane) & 1u)) {
+    // the lanes sample the survivors [pick, ns) at even spacing; one ballot
+    // per corner brackets it between two samples, a binary search finishes
+    const int nsv = ns - pick;
+    const uint32_t ks = nsv > 0 ? keys[pick + ((lane * nsv) >> 5)] : 0xffffffffu;
+    {
         const int cx = (lane & 1) ? px2 : px, cy = (lane & 2) ? py2 : py, cz = (lane & 4) ? pz2 : pz;
         ck = ((uint32_t)cz << xyb) | ((uint32_t)cy << xb) | (uint32_t)cx;
-        int lo = pick, n = ns - pick;
+    }
+    int below = 0;
+#pragma unroll
+    for (int c = 0; c < 8; c++) {
+        const uint32_t kc = __shfl_sync(FULL, ck, c);
+        const int t = __popc(__ballot_sync(FULL, ks < kc));
+        if (lane == c) below = t;
+    }
+    if (lane < 8 && !((cov >> lane) & 1u)) {
+        int lo = below == 0 ? pick : pick + (((below - 1) * nsv) >> 5) + 1;
+        const int hi = below == 32 ? ns : pick + ((below * nsv) >> 5);
+        int n = hi - lo;
         while (n > 0) {
             const int half = n >> 1;
             if (keys[lo + half] < ck) { lo += half + 1; n -= half + 1; }
