@@ -980,20 +980,19 @@ __device__ __forceinline__ int place1(int t, int pp, bool full, uint32_t* mt, in
             const int i = cb + lane;
             const unsigned m = i < nc ? st_feasible(st[i]) : 0u;
             const int c = __popc(m);
-            int inc = c;
-#pragma unroll
-            for (int d = 1; d < 32; d <<= 1) {
-                const int v = __shfl_up_sync(FULL, inc, d);
-                if (lane >= d) inc += v;
-            }
-            const int tot = __shfl_sync(FULL, inc, 31);
+            // lane prefix of the pair counts (each below 8) from their bits
+            const unsigned b0 = __ballot_sync(FULL, c & 1), b1 = __ballot_sync(FULL, c & 2),
+                           b2 = __ballot_sync(FULL, c & 4);
+            const unsigned lt = lanemask_lt();
+            const int excl = __popc(b0 & lt) + 2 * __popc(b1 & lt) + 4 * __popc(b2 & lt);
+            const int tot = __popc(b0) + 2 * __popc(b1) + 4 * __popc(b2);
             if (idx < run + tot) {
-                const unsigned hit = __ballot_sync(FULL, idx < run + inc);
+                const unsigned hit = __ballot_sync(FULL, idx < run + excl + c);
                 const int l = __ffs(hit) - 1;
-                const int excl = __shfl_sync(FULL, inc - c, l);
+                const int ex = __shfl_sync(FULL, excl, l);
                 const unsigned ml = __shfl_sync(FULL, m, l);
                 pick = cb + l;
-                pick_oi = __fns(ml, 0, idx - run - excl + 1);
+                pick_oi = __fns(ml, 0, idx - run - ex + 1);
                 break;
             }
             run += tot;
