@@ -129,6 +129,12 @@ CASES = [
     ("multi_restart_mu", lambda: [synth.multi_restart(2)], [0, 1], 1, ["--mu", "0.45"]),
     ("batched", lambda: synth.batched_set(8), [0, 1, 2, 3], 1, []),
     ("stress", lambda: synth.stress_set(2), [0, 1, 2, 3], 1, []),
+    # every step on the random branch (full evaluation and randrange)
+    ("multi_restart_eps1", lambda: [synth.multi_restart(2)], [0, 1, 2, 3], 1, ["--eps", "1.0"]),
+    # a low acceptance threshold over two passes (fallback flag and pass choice)
+    ("multi_restart_theta05_passes2", lambda: [synth.multi_restart(2)], [5, 6], 2,
+     ["--theta", "0.5", "--eps", "0.5"]),
+    ("batched_input_eps07", lambda: synth.batched_set(8)[:2], [0, 1], 1, ["--order", "input", "--eps", "0.7"]),
 ]
 
 # A seeded 1 % sample of the instances of the bench's batched (4096 instances,
@@ -165,6 +171,8 @@ def python_ref(inst_text, seed, passes, flags):
             kw["eps"] = float(flags[i + 1]); i += 2
         elif f == "--no-theta":
             kw["theta"] = None; i += 1
+        elif f == "--theta":
+            kw["theta"] = float(flags[i + 1]); i += 2
         elif f == "--order":
             kw["order"] = flags[i + 1]; i += 2
         elif f == "--first-fit":

@@ -230,6 +230,8 @@ def flags_to_kw(flags):
             kw["eps"] = float(flags[i + 1]); i += 2
         elif f == "--no-theta":
             kw["theta"] = None; i += 1
+        elif f == "--theta":
+            kw["theta"] = float(flags[i + 1]); i += 2
         elif f == "--order":
             kw["order"] = flags[i + 1]; i += 2
         elif f == "--first-fit":
