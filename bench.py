@@ -155,10 +155,12 @@ def golden_parity(results, opts_seed: int, name: str):
     rows = [json.loads(l) for l in open(GOLDEN)]
     if name == "multi_restart":
         case = next((r for r in rows if r["case"] == "multi_restart"), None)
-        pairs = [(results[0], k, exp) for k, exp in enumerate(case["expected"])] if case else []
+        pairs = [(results[0], k, exp) for k, exp in enumerate(case["expected"])
+                 if k < results[0].restarts] if case else []
         what = "restarts"
     elif name in ("batched", "stress"):
-        pairs = [(results[r["set_index"]], 0, r["expected"][0]) for r in rows if r["case"] == f"{name}_1pct"]
+        pairs = [(results[r["set_index"]], 0, r["expected"][0]) for r in rows
+                 if r["case"] == f"{name}_1pct" and r["set_index"] < len(results)]
         what = "sampled instances (1 %, restart 0)"
     else:
         return None
@@ -308,6 +310,10 @@ def main():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--no-reference-gpu", action="store_true")
+    ap.add_argument("--instances", type=int, default=0,
+                    help="profiling runs: only the workload's first N instances")
+    ap.add_argument("--restarts", type=int, default=0,
+                    help="profiling runs: R restarts per instance instead of the workload's")
     ap.add_argument("--tile", default=None,
                     help="P,C,G,D,M decoder tile instead of the autotuner's choice (profiling runs)")
     args = ap.parse_args()
@@ -340,6 +346,14 @@ def main():
         return float(t.item())
 
     insts_py, opts, desc, R = workload(args.workload, rank)
+    if args.instances > 0 or args.restarts > 0:   # a smaller case of the same workload
+        if args.instances > 0:
+            insts_py = insts_py[:args.instances]
+        if args.restarts > 0:
+            R = args.restarts
+            opts.restarts = R
+            opts.seed = rank * R
+        desc += f" [profiling case: {len(insts_py)} instances x {R} restarts]"
     insts = [P.Instance.parse(i.to_thpack()) for i in insts_py]
     n_items = [i.n_items for i in insts_py]
     h = P.Handle(device=local)
