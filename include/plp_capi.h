@@ -175,9 +175,11 @@ void plp_destroy(plp_handle* h);
  * live-point depth C (per decoder, in shared memory; C a multiple of 32),
  * warps per decoder G, decoders per CTA D and minimum resident CTAs per SM M
  * (which caps registers per thread at 65536 / (32 G D M)). (G, D, M) must be
- * one of (1,1,1) (1,2,1) (1,4,1) (1,4,4) (1,8,1) (1,8,2) (2,1,1) (2,2,1) (2,2,5)
+ * one of (1,1,1) (1,1,12) (1,2,1) (1,4,1) (1,4,4) (1,8,1) (1,8,2) (2,1,1) (2,2,1) (2,2,5)
  * (2,4,1) (2,4,3) (4,1,1) (4,1,5) (4,1,6) (4,2,1) (4,2,3) (4,4,1) (8,1,1)
- * (8,1,3) (8,2,1); 0 keeps the current value. Restarts that outgrow the tile
+ * (8,1,3) (8,2,1); 0 keeps the current value. (1,1,12) holds the decoder to
+ * 160 registers, so three warps fit in each SM partition's register file
+ * where 185 allow two. Restarts that outgrow the tile
  * are re-run with a deeper one, so the tile affects speed only, never results.
  * A new handle starts at P = 256, C = 512, G = 1, D = 1, M = 1. */
 int plp_set_tile(plp_handle* h, int32_t P, int32_t C, int32_t G, int32_t D, int32_t M);
