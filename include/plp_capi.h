@@ -263,11 +263,21 @@ int plp_request_times(plp_handle* h, int64_t request_id, double* queued_s, doubl
  * Both are caller-owned device buffers. The work is enqueued on `stream`
  * (a cudaStream_t, NULL = legacy default stream); synchronise it before
  * reading the outputs. The first call on each device looks up the scratch's
- * device address (cudaGetSymbolAddress); make that first call before any
- * stream capture. Every call shares the scratch, so calls that overlap on the
+ * device address (cudaGetSymbolAddress) and keeps it for the process, so the
+ * entry point cannot be used on a device after cudaDeviceReset.
+ * Host side: the call builds the tables in ordinary (pageable) host memory
+ * that it allocates and frees, and copies them in with cudaMemcpyAsync; a
+ * pageable copy makes the host wait until the bytes are staged, so the call
+ * can block. It is therefore refused (PLP_E_INVALID) while `stream` is being
+ * captured. Every call shares the scratch, so calls that overlap on the
  * GPU race: serialise them (one stream, or wait between calls). Instances
  * whose tables do not fit the scratch (about 8 MiB of restarts x 8 bytes,
- * types x 88 bytes and steps x 4 bytes) return PLP_E_CAPACITY. */
+ * types x 88 bytes and steps x 4 bytes) return PLP_E_CAPACITY.
+ * Errors per restart: err != 0 in a record marks a restart that failed, and
+ * no retry runs (plp_solve reruns such restarts, this call does not): 1 or 2
+ * = tile overflow (not reached: the tile is sized for the instance's step
+ * count), 3 = the randrange rejection bound was hit. Check err in every
+ * record. */
 int plp_decode_noalloc(const plp_instance* inst, const plp_run_opts* opts, void* d_heads,
                        void* d_places, void* stream);
 

@@ -3,9 +3,14 @@
 // and for the CPU baseline timing. Test infrastructure; built into
 // oracle/_ref/ by `make -C oracle ref`.
 //
-//   ref_harness <instance> [--seed S] [--restarts R] [--passes P] [--eps F]
-//               [--theta F | --no-theta] [--order volume|input] [--first-fit]
-//               [--mu F] [--threads T] [--json] [--repeat N]
+//   ref_harness <instance> [<instance> ...] [--seed S] [--restarts R] [--passes P]
+//               [--eps F] [--theta F | --no-theta] [--order volume|input]
+//               [--first-fit] [--mu F] [--threads T] [--json] [--repeat N]
+//
+// Every instance gets restarts seed .. seed + R - 1; the threads share one
+// work list of (instance, restart) pairs, so a sample drawn across a
+// workload's instances is timed with its own mix of sizes. With --json the
+// rows come out instance by instance, restart by restart.
 //
 // Restart k runs plp::run(inst, seed + k, ...) exactly as the reference CLI
 // does for `--single-pass --seed (seed + k)` (gpu/plp_gpu.cpp:131-133). For
@@ -80,7 +85,8 @@ plp::RunResult run_fixed(const plp::Instance& inst, int seed, int passes, double
 }  // namespace
 
 int main(int argc, char** argv) {
-    std::string path, order = "volume";
+    std::vector<std::string> paths;
+    std::string order = "volume";
     int seed = 0, restarts = 1, passes = 1, threads = 1, repeat = 1;
     double eps = plp::EPS_QUALITY, theta = plp::THETA;
     bool no_theta = false, first_fit = false, as_json = false;
@@ -102,32 +108,36 @@ int main(int argc, char** argv) {
         else if (a == "--threads") threads = std::atoi(next().c_str());
         else if (a == "--repeat") repeat = std::atoi(next().c_str());
         else if (a == "--json") as_json = true;
-        else if (!a.empty() && a[0] != '-') path = a;
+        else if (!a.empty() && a[0] != '-') paths.push_back(a);
         else { std::fprintf(stderr, "unknown flag: %s\n", a.c_str()); return 2; }
     }
-    if (path.empty() || restarts < 1 || passes < 1 || threads < 1) {
-        std::fprintf(stderr, "usage: ref_harness <instance> [flags]\n");
+    if (paths.empty() || restarts < 1 || passes < 1 || threads < 1) {
+        std::fprintf(stderr, "usage: ref_harness <instance> [<instance> ...] [flags]\n");
         return 2;
     }
-    plp::Instance inst;
-    try {
-        inst = plp::load_instance(path);
-    } catch (const plp::InstanceFormatError& e) {
-        std::fprintf(stderr, "instance error: %s\n", e.what());
-        return 1;
+    std::vector<plp::Instance> insts(paths.size());
+    for (size_t i = 0; i < paths.size(); i++) {
+        try {
+            insts[i] = plp::load_instance(paths[i]);
+        } catch (const plp::InstanceFormatError& e) {
+            std::fprintf(stderr, "instance error: %s\n", e.what());
+            return 1;
+        }
     }
-    std::vector<plp::RunResult> res(restarts);
+    const long long n_work = (long long)insts.size() * restarts;
+    std::vector<plp::RunResult> res(n_work);
     double total_s = 0;
     for (int rep = 0; rep < repeat; rep++) {
-        std::atomic<int> next_k{0};
+        std::atomic<long long> next_w{0};
         auto t0 = std::chrono::steady_clock::now();
         auto work = [&]() {
             SerialBackend be;
             for (;;) {
-                int k = next_k.fetch_add(1);
-                if (k >= restarts) break;
-                res[k] = run_fixed(inst, seed + k, passes, eps, no_theta ? nullptr : &theta,
-                                   order, first_fit, be);
+                long long w = next_w.fetch_add(1);
+                if (w >= n_work) break;
+                const int k = (int)(w % restarts);
+                res[w] = run_fixed(insts[w / restarts], seed + k, passes, eps,
+                                   no_theta ? nullptr : &theta, order, first_fit, be);
             }
         };
         std::vector<std::thread> pool;
@@ -139,7 +149,7 @@ int main(int argc, char** argv) {
         for (const auto& r : res) std::cout << plp::to_json(r) << "\n";
     } else {
         std::printf("{\"decodes\": %lld, \"seconds\": %.9f, \"threads\": %d}\n",
-                    (long long)restarts * repeat, total_s, threads);
+                    n_work * repeat, total_s, threads);
     }
     return 0;
 }

@@ -2007,6 +2007,13 @@ int plp_decode_noalloc(const plp_instance* inst, const plp_run_opts* opts, void*
     if (opts->engine != 0)
         return set_error(PLP_E_INVALID, "plp_decode_noalloc: extreme-point decoder only (engine 0)");
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    // The tables go in with a copy from ordinary host memory that lives only
+    // for this call: a capture would record that address, so capture is refused.
+    cudaStreamCaptureStatus cap_status = cudaStreamCaptureStatusNone;
+    cudaError_t ce = cudaStreamIsCapturing(st, &cap_status);
+    if (ce != cudaSuccess) return set_cuda_error("plp_decode_noalloc: stream query", ce);
+    if (cap_status != cudaStreamCaptureStatusNone)
+        return set_error(PLP_E_INVALID, "plp_decode_noalloc: not callable during stream capture");
     Batch b;
     int s = b.build({&inst->inst}, {*opts});
     if (s != PLP_OK) return s;
@@ -2020,7 +2027,7 @@ int plp_decode_noalloc(const plp_instance* inst, const plp_run_opts* opts, void*
     t.G = 1;
     t.M = 1;
     t.D = 8;
-    while (t.D > 2 && decoder_smem_bytes(t.P, t.C, b.Hz, t.G) * t.D > 200 * 1024) t.D >>= 1;
+    while (t.D > 1 && decoder_smem_bytes(t.P, t.C, b.Hz, t.G) * t.D > 200 * 1024) t.D >>= 1;
     if (t.P > P_MAX || decoder_smem_bytes(t.P, t.C, b.Hz, t.G) * t.D > 227 * 1024 || 1 + 7 * steps > C_MAX)
         return set_error(PLP_E_CAPACITY, "plp_decode_noalloc: instance too large for the shared-memory tile");
     // scratch: the address is set up on the first call on each device

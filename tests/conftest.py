@@ -8,7 +8,8 @@ import pytest
 REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 PKG = os.path.join(REPO, "plp-gpu_b200")
 GOLDEN = os.path.join(REPO, "tests", "golden")
-REFERENCE = "/root/reference"          # only present where the reference tree is mounted
+# the reference tree, only present where it is mounted
+REFERENCE = os.environ.get("PLP_REFERENCE", "/root/reference")
 for p in (PKG, os.path.join(REPO, "tests")):
     if p not in sys.path:
         sys.path.insert(0, p)

@@ -1,7 +1,11 @@
 #!/usr/bin/env python3
 """Regenerates the golden fixtures in tests/golden/ (run in a container that
-has the reference tree at /root/reference and the reference programs built
-with `make -C oracle ref`).
+has the reference tree at $PLP_REFERENCE, default /root/reference, and the
+reference programs built with `make -C oracle ref`).
+
+    python tests/golden/make_golden.py                        # every fixture
+    python tests/golden/make_golden.py --reference-fixtures   # reference/, br.jsonl,
+                                                              # multi_restart_1024.json
 
 Fixtures:
   selftest_ref.txt   the reference --selftest protocol (4 seeds x 16 random()
@@ -19,6 +23,24 @@ Fixtures:
                      seeded synthetic workloads, time_s removed; every case also
                      cross-checked here against the reference CPython solver
                      (plp.solver.run) on a sample of restarts
+  reference/         the reference's own fixtures, copied byte for byte as test
+                     data: the 19 instance files of data/instances/ and
+                     data/synthetic/SYN1.txt, a reduced data/manifest.json (name,
+                     file, container, type and item counts, item volume), and
+                     the checked-in parity outputs parity/ref_{cpu,host,gpu}/
+                     {BR1,BR2,BR3,SYN1}.json (CPython, g++ and the reference's
+                     plain CUDA build)
+  br.jsonl           the reference g++ build on every manifest instance and SYN1:
+                     seed 0 at --eps 0 --no-theta (the parity gate's mode) in
+                     full, and seeds 0..15 at the default eps 0.3 / theta 0.9 as
+                     row digests (seed 0 in full), time_s removed; the eps-0
+                     rows are cross-checked against CPython
+  multi_restart_1024.json
+                     the multi-restart workload (one 10-type instance) at seeds
+                     0..1023, eps 0.3, theta 0.9, one pass: per restart a digest
+                     of its JSON (time_s removed) with its volume, box count and
+                     score, and the best restart under the reference's selection
+                     rule (gpu/plp_common.hpp:493-511) with its full JSON
 """
 from __future__ import annotations
 
@@ -36,7 +58,10 @@ REPO = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, os.path.join(REPO, "plp-gpu_b200"))
 from plpb200 import synth  # noqa: E402
 
-REF = "/root/reference"
+sys.path.insert(0, os.path.dirname(HERE))
+from parity_gate import row_digest  # noqa: E402
+
+REF = os.environ.get("PLP_REFERENCE", "/root/reference")
 HARNESS = os.path.join(REPO, "oracle", "_ref", "ref_harness")
 PLP_BLOCK = os.path.join(REPO, "oracle", "_ref", "plp_block")
 
@@ -225,7 +250,103 @@ def make_decoder() -> list:
     return rows
 
 
+PARITY_NAMES = ["BR1", "BR2", "BR3", "SYN1"]
+MANIFEST_KEYS = ("name", "file", "container_cm", "n_types", "total_qty", "item_volume_cm3")
+
+
+def copy_reference_fixtures() -> list:
+    """Copies the reference's instance files and parity outputs (test data)."""
+    dst = os.path.join(HERE, "reference")
+    man = json.load(open(os.path.join(REF, "data", "manifest.json")))["instances"]
+    entries = [{k: e[k] for k in MANIFEST_KEYS} for e in man]
+    entries.append({"name": "SYN1", "file": "synthetic/SYN1.txt"})
+    for e in entries:
+        out = os.path.join(dst, "data", e["file"])
+        os.makedirs(os.path.dirname(out), exist_ok=True)
+        with open(os.path.join(REF, "data", e["file"]), "rb") as fi, open(out, "wb") as fo:
+            fo.write(fi.read())
+    with open(os.path.join(dst, "data", "manifest.json"), "w") as f:
+        json.dump({"instances": entries[:-1]}, f, indent=1)
+        f.write("\n")
+    for build in ("ref_cpu", "ref_host", "ref_gpu"):
+        os.makedirs(os.path.join(dst, "parity", build), exist_ok=True)
+        for n in PARITY_NAMES:
+            with open(os.path.join(REF, "parity", build, n + ".json"), "rb") as fi, \
+                    open(os.path.join(dst, "parity", build, n + ".json"), "wb") as fo:
+                fo.write(fi.read())
+    return entries
+
+
+def make_br(entries) -> list:
+    rows = []
+    for e in entries:
+        path = os.path.join(REF, "data", e["file"])
+        text = open(path).read()
+        sha = hashlib.sha256(text.encode()).hexdigest()
+        for case, seeds, flags in (("eps0", [0], ["--eps", "0", "--no-theta"]), ("eps03", list(range(16)), [])):
+            got = harness(path, seeds, 1, flags)
+            row = {"case": case, "name": e["name"], "file": e["file"], "sha256": sha,
+                   "seeds": seeds, "passes": 1, "flags": flags}
+            if case == "eps0":
+                if python_ref(text, 0, 1, flags) != got[0]:
+                    raise SystemExit(f"g++ and CPython reference disagree on {e['name']}")
+                row["expected"] = got
+            else:     # digests keep the fixture small; seed 0 in full for diagnostics
+                row["restarts"] = [[row_digest(r), r["volume_cm3"], r["n_boxes"], r["stability_score"]]
+                                   for r in got]
+                row["first"] = got[0]
+            rows.append(row)
+    return rows
+
+
+def select_best(rows, theta):
+    """Best restart under the reference's rule (gpu/plp_common.hpp:493-511):
+    the accepted packings (score >= theta) if any, else all; highest volume,
+    then more boxes; the earliest wins ties. Returns (index, no restart accepted)."""
+    accepted = [i for i, r in enumerate(rows) if theta is None or r["stability_score"] >= theta]
+    pool = accepted or list(range(len(rows)))
+    best = pool[0]
+    for i in pool[1:]:
+        a, b = rows[i], rows[best]
+        if a["volume_cm3"] > b["volume_cm3"] or (a["volume_cm3"] == b["volume_cm3"] and a["n_boxes"] > b["n_boxes"]):
+            best = i
+    return best, not accepted
+
+
+def make_multi_restart_1024() -> dict:
+    inst = synth.multi_restart(2)
+    text = inst.to_thpack()
+    with tempfile.TemporaryDirectory() as td:
+        path = os.path.join(td, "multi_restart.txt")
+        with open(path, "w") as f:
+            f.write(text)
+        got = harness(path, list(range(1024)), 1, [])
+    for k in (0, 511, 1023):
+        if python_ref(text, k, 1, []) != got[k]:
+            raise SystemExit(f"g++ and CPython reference disagree on multi_restart seed {k}")
+    best, fallback = select_best(got, 0.9)
+    return {"case": "multi_restart_1024", "inst_seed": inst.seed, "sha256": hashlib.sha256(text.encode()).hexdigest(),
+            "seeds": [0, 1023], "eps": 0.3, "theta": 0.9, "passes": 1,
+            "digest": "sha256 of json.dumps(row without time_s, sort_keys=True, separators=(',', ':'))",
+            "restarts": [[row_digest(r), r["volume_cm3"], r["n_boxes"], r["stability_score"]] for r in got],
+            "best": {"index": best, "fallback_over_restarts": fallback, "row": got[best]}}
+
+
+def main_reference_fixtures():
+    rows = make_br(copy_reference_fixtures())
+    with open(os.path.join(HERE, "br.jsonl"), "w") as f:
+        for r in rows:
+            f.write(json.dumps(r, separators=(",", ":")) + "\n")
+    print("wrote", len(rows), "BR cases")
+    with open(os.path.join(HERE, "multi_restart_1024.json"), "w") as f:
+        json.dump(make_multi_restart_1024(), f, separators=(",", ":"))
+        f.write("\n")
+    print("wrote multi_restart_1024.json")
+
+
 def main():
+    if "--reference-fixtures" in sys.argv:
+        return main_reference_fixtures()
     with open(os.path.join(HERE, "selftest_ref.txt"), "w") as f:
         f.write(make_selftest())
     with open(os.path.join(HERE, "rng_vectors.json"), "w") as f:
@@ -242,6 +363,7 @@ def main():
         for r in brows:
             f.write(json.dumps(r, separators=(",", ":")) + "\n")
     print("wrote", len(brows), "block cases")
+    main_reference_fixtures()
 
 
 if __name__ == "__main__":

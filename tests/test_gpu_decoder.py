@@ -4,6 +4,7 @@
 Every restart's JSON (time_s excluded, as parity/compare_parity.py:30-31
 does) must be identical.
 """
+import hashlib
 import json
 import os
 
@@ -255,3 +256,26 @@ def test_multi_wave_batch_matches_oracle():
         for k in range((n * 7) % 13, 50, 13):
             js, _, _ = O.run(oi, seed=20 + k)
             assert O.strip_time(r.json(k)) == O.strip_time(js), (n, k)
+
+
+def test_multi_restart_every_one_of_1024_restarts_and_best_match_reference_host(handle):
+    """The lockstep multi-restart workload in full (10 types, seeds 0..1023,
+    eps 0.3, theta 0.9, one pass): every restart's JSON against the
+    reference g++ build by digest, and the best packing over the 1024
+    restarts under the reference's selection rule (gpu/plp_common.hpp:493-511)
+    in full (tests/golden/multi_restart_1024.json)."""
+    from parity_gate import row_digest
+    g = json.load(open(os.path.join(GOLDEN, "multi_restart_1024.json")))
+    text = synth.multi_restart(2).to_thpack()
+    assert hashlib.sha256(text.encode()).hexdigest() == g["sha256"]
+    r = handle.solve([P.Instance.parse(text)], P.make_opts(seed=0, restarts=1024))[0]
+    got = [json.loads(r.json(k)) for k in range(1024)]
+    bad = [k for k in range(1024) if row_digest(got[k]) != g["restarts"][k][0]]
+    assert not bad, f"{len(bad)} restarts differ, first {bad[:8]}"
+    best, fallback = r.best()
+    assert (best, fallback) == (g["best"]["index"], g["best"]["fallback_over_restarts"])
+    row = got[best]
+    row.pop("time_s")
+    assert row == g["best"]["row"]
+    accepted = [e for e in g["restarts"] if e[3] >= 0.9] or g["restarts"]
+    assert row["volume_cm3"] == max(e[1] for e in accepted)

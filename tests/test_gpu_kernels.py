@@ -120,3 +120,17 @@ def test_device_item_order_matches_host():
         dev = P.item_order(insts, order)
         for inst, d in zip(insts, dev):
             assert d == [t for t, _ in inst.item_sequence(order)]
+
+
+def test_device_item_order_matches_oracle():
+    """Kernel (d) against the oracle's item_sequence (gpu/plp_common.hpp:335-351):
+    the bench's batched and stress instances and the reference's BR instances."""
+    texts = [synth.batched(30000 + i).to_thpack() for i in range(0, 4096, 97)]
+    texts += [synth.stress(40000 + i).to_thpack() for i in range(0, 512, 101)]
+    man = json.load(open(os.path.join(GOLDEN, "reference", "data", "manifest.json")))["instances"]
+    texts += [open(os.path.join(GOLDEN, "reference", "data", e["file"])).read() for e in man]
+    insts = [P.Instance.parse(t) for t in texts]
+    for order, code in (("volume", 0), ("input", 1)):
+        dev = P.item_order(insts, order)
+        for t, d in zip(texts, dev):
+            assert d == [ti for ti, _ in O.OInstance(t).item_sequence(order=code)]

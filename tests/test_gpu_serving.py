@@ -77,3 +77,33 @@ def test_cancel_and_timeouts():
             h.take(10 ** 9)
         assert e.value.status == P.E_NOT_FOUND
         assert h.poll(10 ** 9) == P.E_NOT_FOUND
+
+
+def test_served_results_match_the_oracle_with_restart_budgets_64_256_1024():
+    """Serving-loop requests of the batched workload's sizes with the
+    serving workload's restart budgets {64, 256, 1024}, submitted while
+    others run: sampled restarts of every request against the CPU oracle,
+    and each request's best restart against the selection rule applied to
+    its own restarts."""
+    rng = random.Random(21)
+    reqs = []
+    for i, R in enumerate((64, 256, 1024, 256, 64, 1024)):
+        text = synth.batched(61000 + 37 * i).to_thpack()
+        reqs.append((text, P.Instance.parse(text), P.make_opts(seed=rng.randrange(100000), restarts=R)))
+    with P.Handle() as h:
+        ids = []
+        for _, inst, o in reqs:
+            ids.append(h.submit(inst, o))
+            time.sleep(0.001)
+        for rid in ids:
+            assert h.wait(rid, 300000) == P.OK, P.last_error()
+        results = [h.take(rid) for rid in ids]
+    for (text, _, o), res in zip(reqs, results):
+        oi = O.OInstance(text)
+        R = o.restarts
+        for k in sorted(set(range(0, R, max(1, R // 24))) | {R - 1}):
+            js, _, _ = O.run(oi, seed=o.seed + k)
+            assert O.strip_time(res.json(k)) == O.strip_time(js), (R, k)
+        summ = res.summaries()
+        key = lambda k: (not summ[k].fallback, summ[k].volume, summ[k].n_boxes, -k)
+        assert res.best()[0] == max(range(R), key=key)
