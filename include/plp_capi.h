@@ -291,6 +291,14 @@ int plp_rng_dump(const int64_t* seeds, int32_t n_seeds, int32_t n_random,
 /* the same stream from the host MT19937 (the plain path's generator) */
 int plp_rng_dump_host(const int64_t* seeds, int32_t n_seeds, int32_t n_random,
                       int32_t n_bits, int32_t k_bits, double* out_random, uint32_t* out_bits);
+/* No counterpart in the reference. Test hook of the bounded barrier wait of
+ * the multi-warp decoders (tile G > 1): later launches of this handle give
+ * each wait wait_limit tries of about 10 us (0 = the kernel's own bound, near
+ * 3 s) and, when skip_warp >= 0, warp skip_warp of every decoder leaves out
+ * its first arrive, so that wait runs out. The launch then ends early with
+ * the barrier error and the solve returns PLP_E_DEVICE; the handle stays
+ * usable. plp_debug_sync_bound(h, 0, -1) restores normal launches. */
+int plp_debug_sync_bound(plp_handle* h, int32_t wait_limit, int32_t skip_warp);
 /* device FSR (kernel e): packings given as rows (type, x, y, z, w, d, h);
  * offsets[n_pack + 1] delimit packings. */
 int plp_fsr_score(const int32_t* rows7, const int32_t* offsets, int32_t n_pack, double mu,

@@ -100,6 +100,11 @@ struct TileConfig {
     int G = 1;         // warps per decoder
     int D = 1;         // decoders per CTA
     int M = 1;         // minimum resident CTAs per SM (register cap)
+    // test hook of the bounded barrier wait (plp_debug_sync_bound), multi-warp
+    // decoders only: tries per wait (0 = the kernel's bound) and 1 + the warp
+    // of every decoder that skips its first arrive (0 = none)
+    int sync_limit = 0;
+    int sync_skip = 0;
 };
 
 // Tiles only deepen: a retry that needed a deeper tile is remembered so the
@@ -697,6 +702,8 @@ static DecodeLaunch make_launch(const Batch& b, const TileConfig& t, const int2*
     L.warps_per_decoder = t.G;
     L.decoders_per_cta = t.D;
     L.min_blocks = t.M;
+    L.sync_limit = t.sync_limit;
+    L.sync_skip = t.sync_skip;
     int occ = 1;
     if (tile_occupancy(b, t, &occ) != cudaSuccess || occ < 1) occ = 1;
     L.ctas = (int)std::max<long long>(1, std::min<long long>((n_work + t.D - 1) / t.D, (long long)sms * occ));
@@ -709,7 +716,8 @@ static DecodeLaunch make_launch(const Batch& b, const TileConfig& t, const int2*
 }
 
 bool same_tile(const TileConfig& a, const TileConfig& b) {
-    return a.P == b.P && a.C == b.C && a.G == b.G && a.D == b.D && a.M == b.M;
+    return a.P == b.P && a.C == b.C && a.G == b.G && a.D == b.D && a.M == b.M &&
+           a.sync_limit == b.sync_limit && a.sync_skip == b.sync_skip;
 }
 
 // After-decoder part of an execution: best restart per instance and, for
@@ -1586,6 +1594,17 @@ void plp_destroy(plp_handle* h) {
     for (auto s : h->streams) cudaStreamDestroy(s);
     if (h->sync_stream) cudaStreamDestroy(h->sync_stream);
     delete h;
+}
+
+int plp_debug_sync_bound(plp_handle* h, int32_t wait_limit, int32_t skip_warp) {
+    if (!h) return set_error(PLP_E_INVALID, "plp_debug_sync_bound: null handle");
+    if (wait_limit < 0 || skip_warp < -1 || skip_warp >= 8)
+        return set_error(PLP_E_INVALID, "plp_debug_sync_bound: out of range");
+    std::lock_guard<std::mutex> g(h->sync_mu);
+    std::lock_guard<std::mutex> lk(h->mu);
+    h->tile.sync_limit = wait_limit;
+    h->tile.sync_skip = skip_warp + 1;
+    return PLP_OK;
 }
 
 int plp_set_tile(plp_handle* h, int32_t P, int32_t C, int32_t G, int32_t D, int32_t M) {

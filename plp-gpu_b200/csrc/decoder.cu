@@ -166,6 +166,8 @@ struct DecoderArgs {
     unsigned long long* scratch;   // per resident warp: passes > 1
     const uint32_t* __restrict__ mt_init;
     int P, C, Hz;
+    int sync_limit;                // tries per barrier wait (0 = SYNC_WAIT_LIMIT)
+    int sync_skip;                 // test hook: 1 + the warp that skips its first arrive
 };
 
 
@@ -209,14 +211,17 @@ struct GroupSync {
     unsigned long long* bar;
     int* abort;
     unsigned phase;
+    int limit;          // tries before a wait gives up
+    bool skip_arrive;   // test hook: this warp's next arrive is left out
     // returns false when the launch is aborting (the caller must return)
     __device__ __forceinline__ bool operator()(int lane) {
         __syncwarp();
         if (G == 1) return true;
-        if (lane == 0) mbar_arrive(bar);
+        if (lane == 0 && !skip_arrive) mbar_arrive(bar);
+        skip_arrive = false;
         bool ok = true;
         for (int k = 0; !mbar_try_wait(bar, phase); k++) {
-            if (k >= SYNC_WAIT_LIMIT || ((k & 63) == 63 && *reinterpret_cast<volatile int*>(abort))) {
+            if (k >= limit || ((k & 63) == 63 && *reinterpret_cast<volatile int*>(abort))) {
                 ok = false;
                 break;
             }
@@ -547,7 +552,8 @@ __device__ __forceinline__ void decoder_body(const DecoderArgs& a, unsigned char
     int* ccount = reinterpret_cast<int*>(base + lay.off_cc(a.C));         // per-chunk item counts
     unsigned short* zt = a.Hz ? reinterpret_cast<unsigned short*>(base + lay.off_zt) : nullptr;
     DecShared* sh = reinterpret_cast<DecShared*>(base + lay.off_sh);
-    GroupSync<G> sync{&sh->bar, a.abort, 0u};
+    GroupSync<G> sync{&sh->bar, a.abort, 0u, a.sync_limit > 0 ? a.sync_limit : SYNC_WAIT_LIMIT,
+                      a.sync_skip == g + 1};
 #define PLP_SYNC()                        \
     if (!sync(lane)) {                    \
         if (lane == 0) atomicOr(a.err_flag, 1 << ERR_SYNC); \
@@ -1648,6 +1654,8 @@ static DecoderArgs decoder_args(const DecodeLaunch& L) {
     a.P = L.P;
     a.C = L.C;
     a.Hz = L.Hz;
+    a.sync_limit = L.sync_limit;
+    a.sync_skip = L.sync_skip;
     return a;
 }
 

@@ -32,6 +32,8 @@ struct DecodeLaunch {
     int decoders_per_cta;     // D
     int min_blocks;           // M (register cap through the launch bounds)
     int ctas;
+    int sync_limit;           // test hook: tries per barrier wait (0 = the kernel's bound)
+    int sync_skip;            // test hook: 1 + the warp that skips its first arrive (0 = none)
 };
 
 int decoder_smem_bytes(int P, int C, int Hz, int G, int sup16 = 0);   // sup16: 16-bit contact areas

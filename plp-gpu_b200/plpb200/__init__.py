@@ -107,6 +107,7 @@ def lib():
         "plp_create": (ctypes.c_int, [SZ, I32, P]),
         "plp_destroy": (None, [P]),
         "plp_set_tile": (ctypes.c_int, [P, I32, I32, I32, I32, I32]),
+        "plp_debug_sync_bound": (ctypes.c_int, [P, I32, I32]),
         "plp_autotune": (ctypes.c_int, [P, P, I32, P, I32, I32, P]),
         "plp_batch_graph": (ctypes.c_int, [P]),
         "plp_solve": (ctypes.c_int, [P, P, I32, P, I32, P]),
@@ -338,6 +339,10 @@ class Handle:
 
     def set_tile(self, P: int = 0, C: int = 0, G: int = 0, D: int = 0, M: int = 0):
         _check(lib().plp_set_tile(self._p, P, C, G, D, M), self._p)
+
+    def debug_sync_bound(self, wait_limit: int = 0, skip_warp: int = -1):
+        """Test hook of the multi-warp decoders' bounded barrier wait."""
+        _check(lib().plp_debug_sync_bound(self._p, wait_limit, skip_warp), self._p)
 
     def autotune(self, instances, opts, max_decodes: int = 0) -> tuple:
         """Times candidate tiles on a sample of the workload and keeps the

@@ -9,6 +9,7 @@ import pytest
 
 import oracle_py as O
 import plpb200 as P
+from plpb200 import synth
 
 pytestmark = pytest.mark.gpu
 
@@ -66,3 +67,27 @@ def test_block_engine_edge_cases_match_oracle(handle, name, pick):
     for k in range(12):
         js = O.run_block(oi, seed=9 + k, passes=2, eps=0.4, pick=pick)
         assert O.strip_time(r.json(k)) == O.strip_time(js), (name, k)
+
+
+@pytest.mark.parametrize("G", [2, 4])
+def test_bounded_barrier_wait_gives_up_with_a_device_error(G):
+    """The multi-warp decoder's barrier waits are bounded. With the test hook
+    one warp of every decoder leaves out its first arrive, so each decoder's
+    first wait runs out after 256 tries (about 3 ms at most); the launch ends
+    with the barrier error, the solve returns PLP_E_DEVICE instead of hanging,
+    and the same handle then solves correctly once the hook is cleared."""
+    text = synth.multi_restart(2).to_thpack()
+    inst = P.Instance.parse(text)
+    with P.Handle() as h:
+        h.set_tile(P=128, C=384, G=G, D=1, M=1)
+        h.debug_sync_bound(wait_limit=256, skip_warp=G - 1)
+        with pytest.raises(P.PlpError) as e:
+            h.solve([inst], P.make_opts(seed=0, restarts=8))
+        assert e.value.status == P.E_DEVICE
+        assert "barrier" in str(e.value)
+        h.debug_sync_bound(0, -1)
+        res = h.solve([inst], P.make_opts(seed=0, restarts=8))[0]
+    oi = O.OInstance(text)
+    for k in range(8):
+        js, _, _ = O.run(oi, seed=k)
+        assert O.strip_time(res.json(k)) == O.strip_time(js)
