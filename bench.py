@@ -2,22 +2,31 @@
 """Benchmark of the B200 extreme-point decoder (decodes/sec at bit-exact parity).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload multi_restart|batched|stress|single_pass]
+                    [--workload batched|stress|multi_restart|single_pass|block]
+    python bench.py --workload feas|feas_plain|fsr|item_order     (kernel timings)
 
 A step is one batched solve of the workload: every restart decoded on the
 device (persistent decoder kernel + per-instance best-of selection). The
-default workload is the lockstep multi-restart case: one seeded synthetic
-instance (587 x 233 x 220 cm container, 10 box types, edges U[25,115], flags
-p=0.8, fill [1.0, 1.1]) with 1024 restarts (seeds 0..1023), eps 0.3,
-theta 0.9, one pass each.
+default workload is the batched one, the largest that fits one launch:
+4096 seeded synthetic instances (587 x 233 x 220 cm container, 3-100 box
+types, 30-370 items) with 256 restarts each (1.05 M decodes per step),
+eps 0.3, theta 0.9, one pass each.
 
 Reported: `value` = decodes/s with the instance tables resident on the device
 (CUDA events on the library's stream, max over ranks); `e2e` = the same
 through plp_solve from host objects (tables copied in, every restart's result
-copied out, each step); `roofline` for the decoder kernel against INT32 issue;
+copied out, each step); `roofline` for the decoder kernel against INT32 issue
+(the reference's full-scan work, and the instructions the kernel executes);
 `cpu_baseline` = the reference's own g++ decoder (oracle/_ref/ref_harness,
-compiled from the reference sources) on the host cores; `plain_path` = this
-library's one-launch-per-step path on the same GPU.
+compiled from the reference sources) on the host cores, over a seeded 1 % of
+the workload's instances, with the reference CPython solver's recorded rate
+on the same sample beside it; `plain_path` = this library's
+one-launch-per-step path on the same GPU; `serving` = Poisson request streams
+through the serving loop.
+
+The kernel workloads (feas, feas_plain, fsr, item_order) time the standalone
+kernel entry points on seeded inputs and print one JSON line each; they are
+the commands the ncu summaries of those kernels were taken with.
 
 Multi-GPU (torchrun): each rank decodes its own restarts (seeds offset by
 rank), no data-path collective; scaling is weak.
@@ -28,6 +37,7 @@ import argparse
 import json
 import math
 import os
+import random
 import statistics
 import subprocess
 import sys
@@ -45,6 +55,8 @@ REF_HARNESS = os.path.join(REPO, "oracle", "_ref", "ref_harness")
 REF_GPU = os.path.join(REPO, "oracle", "_ref", "plp_gpu_cuda")
 GOLDEN = os.path.join(REPO, "tests", "golden", "decoder.jsonl")
 PROFILE_INPUTS = os.path.join(REPO, "profiles", "roofline_inputs.txt")
+CPYTHON_RECORD = os.path.join(REPO, "profiles", "cpython_reference_{}_sample.txt")
+KERNEL_WORKLOADS = ("feas", "feas_plain", "fsr", "item_order")
 INT_OPS_PER_AABB = 6   # x, y, z interval tests of one AABB comparison
 
 
@@ -130,10 +142,11 @@ class Clocks:
                 "samples": len(sm), "reasons": sorted(reasons)}
 
 
-def read_profile_inputs() -> dict:
+def read_profile_inputs(path: str = PROFILE_INPUTS) -> dict:
+    """key = value lines of a committed profile summary (# starts a comment)."""
     out = {}
-    if os.path.exists(PROFILE_INPUTS):
-        for line in open(PROFILE_INPUTS):
+    if os.path.exists(path):
+        for line in open(path):
             line = line.strip()
             if line and not line.startswith("#") and "=" in line:
                 k, v = line.split("=", 1)
@@ -174,20 +187,73 @@ def golden_parity(results, opts_seed: int, name: str):
     return f"{ok}/{len(pairs)} {what} bit-identical to the reference g++ build"
 
 
-def cpu_baseline(insts, opts, R, threads):
-    """The reference's own g++ decoder on the host cores (bounded sample)."""
+class CpuSample:
+    """The workload's CPU sample (plpb200.synth.cpu_sample: a seeded 1 % of
+    its instances, the first restarts of each) written to instance files for
+    the reference's g++ harness."""
+
+    def __init__(self, name: str, insts_py, opts):
+        idx, restarts = synth.cpu_sample(name)
+        self.idx = [i for i in idx if i < len(insts_py)] or [0]
+        self.restarts = restarts
+        self.dir = tempfile.TemporaryDirectory()
+        self.paths = []
+        self.items = []
+        for i in self.idx:
+            p = os.path.join(self.dir.name, f"inst_{i}.txt")
+            with open(p, "w") as f:
+                f.write(insts_py[i].to_thpack())
+            self.paths.append(p)
+            self.items.append(insts_py[i].n_items)
+        self.flags = ["--seed", str(opts.seed), "--eps", str(opts.eps)] + (
+            ["--no-theta"] if math.isnan(opts.theta) else ["--theta", str(opts.theta)])
+
+    def describe(self, restarts=None, n_inst=None) -> str:
+        n = len(self.idx) if n_inst is None else n_inst
+        r = self.restarts if restarts is None else restarts
+        items = self.items[:n]
+        return (f"{n} instances (a seeded 1 % of the workload's, {min(items)}-{max(items)} items) x restarts "
+                f"0..{r - 1} = {n * r} decodes")
+
+    def harness(self, threads: int, restarts=None, n_inst=None, repeat=1) -> dict:
+        r = self.restarts if restarts is None else restarts
+        paths = self.paths if n_inst is None else self.paths[:n_inst]
+        cmd = [REF_HARNESS] + paths + ["--restarts", str(r), "--threads", str(threads),
+                                       "--repeat", str(repeat)] + self.flags
+        return json.loads(subprocess.run(cmd, capture_output=True, text=True, check=True).stdout)
+
+    def close(self):
+        self.dir.cleanup()
+
+
+def cpu_baseline(sample: CpuSample, name: str, threads: int):
+    """The reference's own g++ decoder on the host cores over the workload's
+    CPU sample (all threads, and one thread on the first instances), with the
+    reference CPython solver's recorded rate on the same sample beside it."""
     if not os.path.exists(REF_HARNESS):
         return None
-    with tempfile.NamedTemporaryFile("w", suffix=".txt", delete=False) as f:
-        f.write(insts[0].to_thpack())
-        path = f.name
-    sample = min(R, 1024)
-    flags = ["--eps", str(opts.eps)] + (["--no-theta"] if math.isnan(opts.theta) else ["--theta", str(opts.theta)])
-    cmd = [REF_HARNESS, path, "--seed", str(opts.seed), "--restarts", str(sample), "--threads", str(threads),
-           "--repeat", "4"] + flags
-    out = json.loads(subprocess.run(cmd, capture_output=True, text=True, check=True).stdout)
-    os.unlink(path)
-    return out["decodes"] / out["seconds"], out, sample
+    out = sample.harness(threads)
+    cpu = {"value": out["decodes"] / out["seconds"], "unit": "decodes/s", "cores": out["threads"],
+           "kind": "reference",
+           "sample": sample.describe() + f", reference g++ build of gpu/plp_common.hpp on {out['threads']} "
+                                         f"threads ({out['seconds']:.2f} s)"}
+    n1 = min(len(sample.idx), 8)
+    r1 = max(1, min(sample.restarts, 4))
+    one = sample.harness(1, restarts=r1, n_inst=n1)
+    cpu["single_core"] = {"value": one["decodes"] / one["seconds"], "unit": "decodes/s",
+                          "sample": sample.describe(r1, n1) + ", 1 thread"}
+    py = read_profile_inputs(CPYTHON_RECORD.format(name))
+    if py:
+        cpu["python"] = {
+            "value": float(py["cpython_allcores_decodes_per_s"]), "unit": "decodes/s",
+            "cores": int(py["cpython_allcores_cores"]), "kind": "reference",
+            "single_core": float(py["cpython_1core_decodes_per_s"]),
+            "sample": py["cpython_allcores_sample"] + "; 1 core: " + py["cpython_1core_sample"],
+            "where": f"recorded in the build container ({py['host']}) by oracle/time_cpython.py: the "
+                     "reference's CPython solver does not travel to the GPU host; the g++ build timed there "
+                     f"ran at {py['gpp_allcores_decodes_per_s']} decodes/s on the same sample and cores",
+            "source": os.path.relpath(CPYTHON_RECORD.format(name), REPO)}
+    return cpu
 
 
 def reference_gpu(inst_py, opts):
@@ -217,41 +283,42 @@ def reference_gpu(inst_py, opts):
 
 
 def run_reference(args):
-    """--impl reference: the reference's g++ decoder, all host threads."""
+    """--impl reference: the reference's g++ decoder (its gpu/plp_common.hpp,
+    built from its sources as oracle/_ref/ref_harness) on all host threads,
+    each step one pass over the workload's CPU sample."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
+        return 0
+    if args.workload in KERNEL_WORKLOADS or args.workload == "block":
+        print(json.dumps({"impl": "reference", "unavailable": f"no reference decoder arm for {args.workload}"}))
         return 0
     insts, opts, desc, R = workload(args.workload, 0)
     threads = os.cpu_count() or 1
     if not os.path.exists(REF_HARNESS):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_harness not built"}))
         return 0
-    with tempfile.NamedTemporaryFile("w", suffix=".txt", delete=False) as f:
-        f.write(insts[0].to_thpack())
-        path = f.name
-    sample = min(R, 1024)
-    flags = ["--eps", str(opts.eps)] + (["--no-theta"] if math.isnan(opts.theta) else ["--theta", str(opts.theta)])
-    cmd = [REF_HARNESS, path, "--seed", str(opts.seed), "--restarts", str(sample), "--threads", str(threads)] + flags
+    sample = CpuSample(args.workload, insts, opts)
     for _ in range(args.warmup):
-        subprocess.run(cmd, capture_output=True, check=True)
-    secs = []
+        sample.harness(threads)
+    secs, decodes = [], 0
     for _ in range(args.steps):
-        out = json.loads(subprocess.run(cmd, capture_output=True, text=True, check=True).stdout)
+        out = sample.harness(threads)
         secs.append(out["seconds"])
-    os.unlink(path)
+        decodes += out["decodes"]
     total = sum(secs)
-    value = sample * args.steps / total
+    value = decodes / total
     line = {
         "impl": "reference", "metric": "decodes/sec", "value": value, "unit": "decodes/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1000 * total / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "int32+f64", "data": "synthetic (seeded generator)",
-        "config": {"workload": desc, "sample_restarts_per_step": sample},
+        "config": {"workload": desc, "sample_decodes_per_step": decodes // args.steps},
         "cpu_baseline": {"value": value, "unit": "decodes/s", "cores": threads, "kind": "reference",
-                         "sample": f"{sample} restarts of the workload per step, reference g++ "
-                                   f"(gpu/plp_common.hpp) on {threads} threads"},
+                         "sample": sample.describe() + f" per step, reference g++ (gpu/plp_common.hpp) on "
+                                                       f"{threads} threads"},
         "e2e": {"value": value, "unit": "decodes/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    sample.close()
     print(json.dumps(line))
     return 0
 
@@ -298,14 +365,83 @@ def serving_report(device: int, rates=(100, 1000, 10000), window_s=2.0, max_requ
     return out
 
 
+# ---------------------------------------------------------------------------
+# kernel timings (--workload feas|feas_plain|fsr|item_order): the standalone
+# kernel entry points on seeded inputs, best wall time of a few calls
+# ---------------------------------------------------------------------------
+def _best(fn, reps=5):
+    fn()
+    best = float("inf")
+    for _ in range(reps):
+        t = time.perf_counter()
+        fn()
+        best = min(best, time.perf_counter() - t)
+    return best
+
+
+def feas_bench(n_cand=4096, n_boxes=512, seed=3):
+    """One feasibility step of stress size: n_cand extreme points x 6
+    orientations against n_boxes placed boxes stacked in a 587x233x220
+    container (non-overlapping boxes on a grid of columns)."""
+    rng = random.Random(seed)
+    L, W, H = 587, 233, 220
+    boxes = []
+    cols = [(x, y) for x in range(0, L - 40, 41) for y in range(0, W - 40, 41)]
+    rng.shuffle(cols)
+    for i in range(n_boxes):
+        x, y = cols[i % len(cols)]
+        z = 11 * (i // len(cols))
+        boxes.append((x, y, z, x + rng.randint(10, 40), y + rng.randint(10, 40), z + rng.randint(5, 11)))
+    cand = sorted({(rng.randrange(L), rng.randrange(W), rng.randrange(H)) for _ in range(n_cand)},
+                  key=lambda p: (p[2], p[1], p[0]))
+    ors = [(37, 21, 15), (21, 37, 15), (37, 15, 21), (15, 37, 21), (21, 15, 37), (15, 21, 37)]
+    t = _best(lambda: P.feas_check_all(cand, ors, boxes, L, W, H))
+    return {"kernel": "feas_kernel", "entry": "plp_feas_check_all", "candidates": len(cand),
+            "orientations": 6, "boxes": n_boxes, "ms_per_call": t * 1e3}
+
+
+def feas_plain_bench(restarts=2):
+    """The plain path on the multi_restart instance: one launch per item step."""
+    inst = P.Instance.parse(synth.multi_restart(2).to_thpack())
+    t = _best(lambda: P.run_plain(inst, seed=0, restarts=restarts), reps=2)
+    return {"kernel": "feas_kernel", "entry": "plp_run_plain", "restarts": restarts,
+            "ms_per_decode": t * 1e3 / restarts}
+
+
+def fsr_bench(n_inst=64, restarts=64):
+    """FSR of n_inst x restarts packings decoded from the batched workload."""
+    insts = [P.Instance.parse(i.to_thpack()) for i in synth.batched_set(n_inst)]
+    with P.Handle() as h:
+        res = h.solve(insts, P.make_opts(seed=0, restarts=restarts))
+    packs = [r.placements(k) for r in res for k in range(r.restarts)]
+    t = _best(lambda: P.fsr_score(packs))
+    return {"kernel": "fsr_kernel", "entry": "plp_fsr_score", "packings": len(packs),
+            "boxes": int(sum(len(p) for p in packs)), "ms_per_call": t * 1e3}
+
+
+def item_order_bench(n_inst=4096):
+    """Item order (kernel d) of the batched workload's instances."""
+    insts = [P.Instance.parse(i.to_thpack()) for i in synth.batched_set(n_inst)]
+    t = _best(lambda: P.item_order(insts))
+    return {"kernel": "item_order_kernel", "entry": "plp_item_order", "instances": n_inst,
+            "items": int(sum(i.info()[2] for i in insts)), "ms_per_call": t * 1e3}
+
+
+def kernel_bench(name: str) -> int:
+    fn = {"feas": feas_bench, "feas_plain": feas_plain_bench, "fsr": fsr_bench,
+          "item_order": item_order_bench}[name]
+    print(json.dumps(fn()))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", default="multi_restart",
-                    choices=["multi_restart", "batched", "stress", "single_pass", "block"])
+    ap.add_argument("--workload", default="batched",
+                    choices=["batched", "stress", "multi_restart", "single_pass", "block"] + list(KERNEL_WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
@@ -319,6 +455,8 @@ def main():
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload in KERNEL_WORKLOADS:
+        return kernel_bench(args.workload)
     if args.warmup < 3:
         raise SystemExit("--warmup must be >= 3")
 
@@ -384,9 +522,9 @@ def main():
     t_mean = sum(T) / len(T)
     placed = [r.summary(k).n_boxes for r, k in sample]
     pairs = [w[1] for w in work]
-    dist = {"placed_per_decode": [min(placed), sum(placed) / len(placed), max(placed)],
-            "pairs_per_decode": [min(pairs), sum(pairs) / len(pairs), max(pairs)],
-            "sampled_decodes": len(sample)}
+    distributions = {"placed_per_decode": [min(placed), sum(placed) / len(placed), max(placed)],
+                     "pairs_per_decode": [min(pairs), sum(pairs) / len(pairs), max(pairs)],
+                     "sampled_decodes": len(sample)}
     del sample
     del slots, warm_results   # their pinned result block goes back to the handle's pool
     clocks = Clocks(local)
@@ -435,20 +573,42 @@ def main():
     if rank == 0:
         peaks = measured_peaks()
         props = torch.cuda.get_device_properties(local)
-        sm_max = float(peaks.get("sm_max_mhz", 1965.0))
+        if "sm_max_mhz" in peaks:
+            sm_max, sm_src = float(peaks["sm_max_mhz"]), "sm_max_mhz of MEASURED_PEAKS.json"
+        elif clk.get("sm_max_mhz"):
+            sm_max, sm_src = float(clk["sm_max_mhz"]), "clocks.max.sm sampled by nvidia-smi in this run"
+        else:
+            sm_max, sm_src = 1965.0, "the B200's nominal clocks.max.sm (no clock record)"
         int_peak = props.multi_processor_count * 128 * sm_max * 1e6 / 1e12   # T int-op/s
         dec_mean_ms = sum(dec_ms) / len(dec_ms)
-        achieved = t_mean * R * len(insts) * INT_OPS_PER_AABB / (dec_mean_ms / 1000.0) / 1e12
+        decodes_per_launch = R * len(insts)
+        achieved = t_mean * decodes_per_launch * INT_OPS_PER_AABB / (dec_mean_ms / 1000.0) / 1e12
         prof = read_profile_inputs()
         traffic = prof.get(f"traffic_bytes_per_launch.{args.workload}")
         if args.workload == "block":   # no reference work replay for the block engine
             achieved = None
+        # the instructions the kernel really executes: thread instructions per
+        # decode from the committed ncu capture of a smaller case of the same
+        # workload, times this launch's decodes, over the decoder's own time
+        executed = None
+        tin = prof.get(f"thread_inst_per_decode.{args.workload}")
+        if tin:
+            ex = float(tin) * decodes_per_launch / (dec_mean_ms / 1000.0) / 1e12
+            executed = {"achieved": ex, "peak": int_peak, "unit": "T thread-inst/s", "frac": ex / int_peak,
+                        "thread_inst_per_decode": float(tin),
+                        "source": prof.get(f"thread_inst_source.{args.workload}"),
+                        "note": "every executed thread instruction (integer, FP64, memory, control) counted "
+                                "against one instruction per INT32 lane per clock: the hardware's own "
+                                "occupancy of the issue peak"}
         roofline = {
             "bound": "int32", "achieved": achieved, "peak": int_peak, "unit": "Tint-op/s",
             "frac": achieved / int_peak if achieved is not None else None,
+            "frac_kind": "reference-work equivalent: the reference's full-scan AABB work per decode "
+                         "delivered per second, over the INT32 issue peak (executed: the hardware's own "
+                         "fraction)",
+            "executed": executed,
             "traffic": float(traffic) if traffic else None,
-            "peak_source": f"{props.multi_processor_count} SMs x 128 INT32 lanes x {sm_max:.0f} MHz "
-                           "(sm_max_mhz of MEASURED_PEAKS.json)",
+            "peak_source": f"{props.multi_processor_count} SMs x 128 INT32 lanes x {sm_max:.0f} MHz ({sm_src})",
             "work_unit": f"reference AABB tests per decode T = {t_mean:.0f} (mean over {len(T)} of the "
                          f"step's restarts, evenly spaced) x {INT_OPS_PER_AABB} int ops",
             "issue_active_pct_ncu": float(prof[f"issue_active_pct.{args.workload}"])
@@ -462,17 +622,10 @@ def main():
             "kernel_ms_per_launch": dec_mean_ms,
         }
         cpu = None
-        if not args.no_cpu_baseline:
-            cb = cpu_baseline(insts_py, opts, R, os.cpu_count() or 1)
-            if cb:
-                v, raw, sample = cb
-                cpu = {"value": v, "unit": "decodes/s", "cores": raw["threads"], "kind": "reference",
-                       "sample": f"{sample} restarts x 4 repeats of the workload's first instance, reference "
-                                 f"g++ build of gpu/plp_common.hpp, {raw['threads']} threads"}
-                one = cpu_baseline(insts_py, opts, min(R, 128), 1)
-                if one:
-                    cpu["single_core"] = {"value": one[0], "unit": "decodes/s",
-                                          "sample": f"{one[2]} restarts x 4 repeats, 1 thread"}
+        if not args.no_cpu_baseline and args.workload != "block":
+            sample = CpuSample(args.workload, insts_py, opts)
+            cpu = cpu_baseline(sample, args.workload, os.cpu_count() or 1)
+            sample.close()
         plain = None
         if not args.no_plain:
             n_pl = 8
@@ -498,7 +651,7 @@ def main():
             "data": "synthetic (seeded generator, 587x233x220 container)",
             "config": {"workload": desc, "instances": len(insts), "restarts": R,
                        "items_per_instance": [min(n_items), max(n_items)],
-                       "distributions": {**dist, "note": "min, mean, max over the sampled decodes; pairs = "
+                       "distributions": {**distributions, "note": "min, mean, max over the sampled decodes; pairs = "
                                                          "(extreme point, orientation) pairs the reference "
                                                          "evaluates per decode"},
                        "parallelism": f"dp{world} (restarts sharded by rank)",

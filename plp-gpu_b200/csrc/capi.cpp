@@ -260,7 +260,7 @@ struct Batch {
     size_t bytes = 0;
     size_t o_desc, o_steps, o_types, o_bcat, o_btab, o_work, o_next, o_heads, o_places, o_best, o_scratch, o_gather, o_redo;
     const uint32_t* mt_init = nullptr;
-    cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     char* h_flag = nullptr;                // pinned error-flag word
     bool own_ctx = true;                   // h_flag and ev allocated by this batch
     std::vector<int2> redo_host;
@@ -477,7 +477,7 @@ struct Pinned {
     // batches (pinned allocation and event creation cost more than a solve's
     // whole host side)
     char* flag = nullptr;
-    cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     // outgrown buffers, freed with the context: freeing pinned memory
     // synchronises the device, which would stall other streams mid-run
     std::vector<char*> retired;
@@ -646,7 +646,7 @@ int batch_prepare(Batch& b, cudaStream_t st, Pinned& pin, int sms, const TileCon
         if (e != cudaSuccess) return fail("pinned flag", e);
         b.own_ctx = false;
         b.h_flag = pin.flag;
-        for (int k = 0; k < 3; k++) b.ev[k] = pin.ev[k];
+        for (int k = 0; k < 4; k++) b.ev[k] = pin.ev[k];
     } else {
         for (auto& ev : b.ev) {
             e = cudaEventCreate(&ev);
@@ -810,8 +810,8 @@ int pending_bits(const Batch& b, bool staged) {
 
 // Records a clean execution of the batch with tile t as one CUDA graph:
 // error-flag reset, the persistent decoder, the retry stage where it applies,
-// the flag copy to the pinned words, selection and gather, with event ev[1]
-// after the first decoder. A capture that fails leaves the batch on direct
+// the flag copy to the pinned words, selection and gather, with events ev[3]
+// and ev[1] around the first decoder (the decoder's own time under replay). A capture that fails leaves the batch on direct
 // launches.
 void batch_capture(Batch& b, cudaStream_t st, int sms, const TileConfig& t) {
     if (b.gexec) {
@@ -842,6 +842,7 @@ void batch_capture(Batch& b, cudaStream_t st, int sms, const TileConfig& t) {
     }
     int n = 0;
     cudaError_t e = cudaMemsetAsync(d_flag, 0, 16, st);
+    if (e == cudaSuccess) e = cudaEventRecord(b.ev[3], st);
     if (e == cudaSuccess) e = enqueue_decoder(L, st);
     if (e == cudaSuccess) n++;
     if (e == cudaSuccess) e = cudaEventRecord(b.ev[1], st);
@@ -938,7 +939,7 @@ int batch_execute(Batch& b, cudaStream_t st, int sms, TileConfig& tile, ExecStat
         if (pending_bits(b, b.gstaged) == 0) {
             float ms = 0, dms = 0;
             cudaEventElapsedTime(&ms, b.ev[0], b.ev[2]);
-            if (cudaEventElapsedTime(&dms, b.ev[0], b.ev[1]) != cudaSuccess) {
+            if (cudaEventElapsedTime(&dms, b.ev[3], b.ev[1]) != cudaSuccess) {
                 cudaGetLastError();
                 dms = ms;
             }

@@ -130,3 +130,21 @@ def serving_stream(n_requests: int, rate_per_s: float, seed: int = 50000):
         t += rng.expovariate(rate_per_s)
         out.append((t, batched(seed + 1 + i), rng.choice((64, 256, 1024))))
     return out
+
+
+def cpu_sample(workload: str):
+    """The bounded sample of a workload that the CPU baselines time: a seeded
+    1 % of its instances (at least one) with the first restarts of each, so
+    the sample keeps the workload's mix of sizes. Returns (indices into the
+    workload's instance list, restarts per instance); restart seeds start at 0
+    as in the workload. The same indices are the 1 % parity sample of the
+    batched and stress workloads."""
+    if workload == "batched":
+        return sorted(random.Random(7).sample(range(4096), 41)), 32
+    if workload == "stress":
+        return sorted(random.Random(8).sample(range(512), 5)), 128
+    if workload == "multi_restart":
+        return [0], 1024
+    if workload == "single_pass":
+        return [0], 1
+    raise ValueError(f"no CPU sample for workload {workload}")

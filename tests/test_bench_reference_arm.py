@@ -29,7 +29,10 @@ def test_reference_arm_prints_the_contract_line():
     assert d["e2e"] == {"value": d["value"], "unit": "decodes/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
     cb = d["cpu_baseline"]
     assert cb["kind"] == "reference" and cb["value"] == d["value"] and cb["cores"] >= 1 and cb["sample"]
-    assert "multi_restart" in d["config"]["workload"]
+    assert d["config"]["workload"].startswith("batched")
+    # a seeded 1 % of the workload's instances, not its first instance alone
+    assert d["config"]["sample_decodes_per_step"] == 41 * 32
+    assert "41 instances" in cb["sample"]
 
 
 def test_reference_arm_other_ranks_stay_silent():
