@@ -135,9 +135,19 @@ cudaError_t tile_occupancy(const Batch& b, const TileConfig& t, int* occ);
 // the type's largest count; the placement rank of every shape (block volume
 // desc, type, orientation, k desc, a desc, b desc) and the shapes by rank; the
 // type order (volume desc, index) and the copies per type.
-int build_block_tables(const Instance& I, const std::vector<TypeOrs>& ors, const plp_run_opts& o,
-                       std::vector<BlkShape>& cat_all, std::vector<int>& tab, InstDesc& d) {
-    const int amax = std::max(1, o.blk_amax), bmax = std::max(1, o.blk_bmax), kmax = std::max(1, o.blk_kmax);
+struct BlockTables {
+    std::vector<BlkShape> cat;
+    std::vector<int> tab;
+    // offsets into tab
+    int bo_order = 0, bo_qty = 0, bo_list_off = 0, bo_list = 0, bo_start_off = 0, bo_start = 0,
+        bo_shape_of_rank = 0;
+    size_t bytes() const { return cat.size() * sizeof(BlkShape) + tab.size() * sizeof(int); }
+};
+
+int make_block_tables(const Instance& I, const std::vector<TypeOrs>& ors, int amax, int bmax, int kmax,
+                      BlockTables& out) {
+    std::vector<int>& tab = out.tab;
+    BlockTables& d = out;
     const int nt = (int)I.types.size();
     std::vector<BlkShape> cat;
     for (int ti = 0; ti < nt; ti++) {
@@ -191,7 +201,6 @@ int build_block_tables(const Instance& I, const std::vector<TypeOrs>& ors, const
         if (vx != vy) return vx > vy;
         return x < y;
     });
-    d.n_types = nt;
     d.bo_order = (int)tab.size();
     tab.insert(tab.end(), tord.begin(), tord.end());
     d.bo_qty = (int)tab.size();
@@ -225,9 +234,82 @@ int build_block_tables(const Instance& I, const std::vector<TypeOrs>& ors, const
     }
     d.bo_shape_of_rank = (int)tab.size();
     tab.insert(tab.end(), by_rank.begin(), by_rank.end());
+    out.cat = std::move(cat);
+    return PLP_OK;
+}
+
+// The tables depend only on the container, the types and (amax, bmax, kmax),
+// so they are kept per process (up to PLP_BLOCK_CACHE_MB, default 1024 MiB,
+// oldest first out): a batch that solves the same instances again appends
+// them instead of rebuilding the catalogue and its sorts.
+std::shared_ptr<const BlockTables> block_tables(const Instance& I, const std::vector<TypeOrs>& ors,
+                                                 int amax, int bmax, int kmax, int* status) {
+    static std::mutex mu;
+    static std::unordered_map<std::string, std::shared_ptr<const BlockTables>> cache;
+    static std::deque<std::string> order;
+    static size_t held = 0;
+    static const size_t limit = [] {
+        size_t mb = 1024;
+        if (const char* v = std::getenv("PLP_BLOCK_CACHE_MB")) {
+            char* end = nullptr;
+            const unsigned long long x = std::strtoull(v, &end, 10);
+            if (end != v) mb = (size_t)x;
+        }
+        return mb << 20;
+    }();
+    std::string key;
+    key.reserve(32 + I.types.size() * 28);
+    auto put = [&](int v) { key.append(reinterpret_cast<const char*>(&v), sizeof v); };
+    for (int v : {I.L, I.W, I.H, amax, bmax, kmax, (int)I.types.size()}) put(v);
+    for (const auto& t : I.types)
+        for (int v : {t.l, (int)t.lf, t.w, (int)t.wf, t.h, (int)t.hf, t.qty}) put(v);
+    {
+        std::lock_guard<std::mutex> g(mu);
+        auto it = cache.find(key);
+        if (it != cache.end()) {
+            *status = PLP_OK;
+            return it->second;
+        }
+    }
+    auto bt = std::make_shared<BlockTables>();
+    *status = make_block_tables(I, ors, amax, bmax, kmax, *bt);
+    if (*status != PLP_OK) return nullptr;
+    std::lock_guard<std::mutex> g(mu);
+    if (bt->bytes() <= limit && !cache.count(key)) {
+        while (held + bt->bytes() > limit && !order.empty()) {
+            auto old = cache.find(order.front());
+            held -= old->second->bytes();
+            cache.erase(old);
+            order.pop_front();
+        }
+        cache.emplace(key, bt);
+        order.push_back(key);
+        held += bt->bytes();
+    }
+    return bt;
+}
+
+// Appends one instance's block tables to the batch's catalogue and table,
+// with its descriptor's offsets.
+int build_block_tables(const Instance& I, const std::vector<TypeOrs>& ors, const plp_run_opts& o,
+                       std::vector<BlkShape>& cat_all, std::vector<int>& tab, InstDesc& d) {
+    int status = PLP_OK;
+    const auto bt = block_tables(I, ors, std::max(1, o.blk_amax), std::max(1, o.blk_bmax),
+                                 std::max(1, o.blk_kmax), &status);
+    if (!bt) return status;
+    const int base = (int)tab.size();
+    d.n_types = (int)I.types.size();
+    d.bo_order = base + bt->bo_order;
+    d.bo_qty = base + bt->bo_qty;
+    d.bo_list_off = base + bt->bo_list_off;
+    d.bo_list = base + bt->bo_list;
+    d.bo_start_off = base + bt->bo_start_off;
+    d.bo_start = base + bt->bo_start;
+    d.bo_shape_of_rank = base + bt->bo_shape_of_rank;
     d.cat_off = (int)cat_all.size();
-    d.n_cat = nc;
-    cat_all.insert(cat_all.end(), cat.begin(), cat.end());
+    d.n_cat = (int)bt->cat.size();
+    tab.insert(tab.end(), bt->tab.begin(), bt->tab.end());
+    cat_all.insert(cat_all.end(), bt->cat.begin(), bt->cat.end());
     d.blk_topk = std::max(1, o.blk_topk);
     d.blk_pick = o.blk_pick;
     if (tab.size() > (size_t)INT_MAX / 2 || cat_all.size() > (size_t)INT_MAX / 2)

@@ -85,3 +85,21 @@ def test_block_engine_batch_rejects_mixed_engines(handle):
     inst = P.Instance.parse(synth.single_pass(1).to_thpack())
     with pytest.raises(P.PlpError):
         handle.solve([inst, inst], [P.make_opts(seed=0), _opts(0)])
+
+
+def test_block_tables_cached_across_solves_stay_exact(handle):
+    """The per-instance block tables are built once per (container, types,
+    amax, bmax, kmax) and appended on later solves, at any position of a
+    batch; the second solve (reordered, another configuration in between)
+    equals the oracle."""
+    texts = [i.to_thpack() for i in synth.batched_set(4, 35000)]
+    insts = [P.Instance.parse(t) for t in texts]
+    first = handle.solve(insts, _opts(2, restarts=3))
+    handle.solve(insts[:2], _opts(2, restarts=3, amax=2, bmax=2, kmax=2))
+    again = handle.solve(list(reversed(insts)), _opts(2, restarts=3))
+    for t, a, b in zip(texts, first, reversed(again)):
+        oi = O.OInstance(t)
+        for k in range(3):
+            exp = O.strip_time(O.run_block(oi, seed=2 + k))
+            assert O.strip_time(a.json(k)) == exp
+            assert O.strip_time(b.json(k)) == exp
