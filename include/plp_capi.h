@@ -246,6 +246,24 @@ int plp_cancel(plp_handle* h, int64_t request_id);
 /* seconds from submit to finish, and to start on the device */
 int plp_request_times(plp_handle* h, int64_t request_id, double* queued_s, double* total_s);
 
+/* No counterpart in the reference. Requests that run the extreme-point decoder
+ * for one pass with every restart kept (engine 0, passes 1, no time limit,
+ * not best_only) are served by one persistent decoder launch that they join
+ * while it runs: each request's tables go into a device arena (half the
+ * budget, at most PLP_SERVE_ARENA_MB, default 4096 MiB, reserved from the
+ * budget on the first such request), its restarts into a device work ring,
+ * and the decoder that finishes its last restart selects its best restart on
+ * the device. Other requests run in waves on worker streams. PLP_SERVE=0 in
+ * the environment when the first request arrives sends every request to the
+ * waves. While the serving launch runs it holds the SMs: a synchronous solve
+ * on the same GPU runs once the launch has stopped (about 5 ms after the last
+ * request finished). This call reports the handle's serving launches,
+ * requests served by them, requests re-run on the wave path's code after a
+ * restart outgrew the serving tile, and eligible requests sent to the waves
+ * (larger than the arena). */
+int plp_serve_counters(plp_handle* h, int64_t* launches, int64_t* served, int64_t* fallbacks,
+                       int64_t* waved);
+
 /* ------------------------------------------------------------------------ */
 /* allocation-free decode                                                    */
 /* ------------------------------------------------------------------------ */

@@ -1236,6 +1236,10 @@ struct Request {
     double t_submit = 0, t_start = 0, t_done = 0;
 };
 
+namespace {
+struct ServeEngine;
+}
+
 struct plp_handle {
     int device = 0;
     int sms = 148;
@@ -1260,6 +1264,11 @@ struct plp_handle {
     std::mutex sync_mu;
     Pinned sync_pin;
     std::shared_ptr<HostPool> pool = std::make_shared<HostPool>();   // result blocks of synchronous solves
+    // serving engine (one persistent launch that requests join), made on the
+    // first eligible request; off with PLP_SERVE=0 or when it cannot be set up
+    ServeEngine* serve = nullptr;
+    bool serve_off = false;
+    std::mutex serve_mu;
 };
 
 namespace {
@@ -1372,6 +1381,652 @@ void worker_main(plp_handle* h, int wi) {
         h->cv.notify_all();
         h->cv_sched.notify_all();
     }
+}
+
+// ===========================================================================
+// serving engine: one persistent decoder launch that requests join while it
+// runs (continuous batching)
+// ===========================================================================
+// A request is eligible when it runs the extreme-point decoder for one pass
+// with every restart's result kept (engine 0, passes 1, no time budget, not
+// best-only); the others go to the wave workers above. An eligible request:
+//   1. is admitted when its tables and results fit the serving arena (a ring
+//      of device memory reserved from the handle's budget: half of it, at
+//      most PLP_SERVE_ARENA_MB, default 4096) and a completion record is free;
+//   2. has, in one stream pass on the upload stream, its descriptor, step
+//      types and orientations copied into its arena region, its restarts
+//      appended to the device work ring, and then the ring's tail advanced
+//      (stream order puts the tables in memory before the tail moves);
+//   3. is decoded by whichever decoders of the running launch claim its items;
+//      the decoder that finishes its last restart selects the best restart and
+//      writes it, with the request's sequence number, to the request's
+//      host-mapped completion record;
+//   4. has its slot heads and placements copied out once the record shows its
+//      sequence number, and completes; its arena region is then free.
+// The launch keeps running while requests arrive. The host stops it after
+// SERVE_IDLE_STOP_S without requests and starts it again for the next one; a
+// decoder that finds no work for about a second exits by itself as well
+// (bounded polling). A request that the running launch's configuration cannot
+// take (a container taller than its top-z index covers, or footprints too
+// large for its 16-bit contact areas) waits until the launch has drained, and
+// the next launch takes the merged configuration. Restarts that overflow the
+// serving tile (P = 256 boxes, C = 768 live points; rare) make their request
+// run again on the wave path's code, which retries with deeper tiles.
+constexpr int SERVE_RING = 1 << 20;            // work items in flight at most
+constexpr int SERVE_RECORDS = 1 << 16;         // requests in flight at most
+constexpr double SERVE_IDLE_STOP_S = 0.005;
+constexpr int SERVE_IDLE_POLLS = 250000;       // about 1 s of empty polls per decoder
+
+size_t serve_align(size_t x, size_t unit) {    // a multiple of unit and of 128 bytes
+    size_t q = unit;
+    while (q % 128) q += unit;
+    return (x + q - 1) / q * q;
+}
+
+struct ServeConfig {
+    int P = 256, C = 768, D = 1, M = 1, Hz = 0, sup16 = 0;
+    bool valid = false;
+};
+
+// absolute arena offsets of one request's tables and results
+struct ServeRegion {
+    size_t off = 0, end = 0;
+    size_t desc = 0, steps = 0, types = 0, heads = 0, places = 0;
+};
+
+bool serve_layout(const Batch& b, size_t pos, size_t limit, ServeRegion& g) {
+    const InstDesc& d = b.desc[0];
+    g.off = pos;
+    g.desc = serve_align(pos, sizeof(InstDesc));
+    g.steps = serve_align(g.desc + sizeof(InstDesc) + sizeof(ServeTail), sizeof(int));
+    g.types = serve_align(g.steps + std::max<size_t>(1, b.steps.size()) * sizeof(int), sizeof(TypeOrs));
+    g.heads = serve_align(g.types + std::max<size_t>(1, b.types.size()) * sizeof(TypeOrs), sizeof(SlotHead));
+    g.places = serve_align(g.heads + (size_t)d.restarts * sizeof(SlotHead), 8);
+    g.end = g.places + (size_t)d.restarts * d.place_stride * 8;
+    return g.end <= limit;
+}
+
+struct ServeJob {
+    int64_t id = 0;
+    Instance inst;                 // copies: the request may be cancelled and taken before admission
+    plp_run_opts opts{};
+    Request* r = nullptr;          // set at admission, when the request can no longer be taken
+    Batch b;
+    bool built = false;
+    int state = 0;                 // 1 published, 2 copying results out
+    ServeRegion g;
+    long long region = -1;         // id of its arena region
+    long long seq = 0;
+    int slot = -1;
+    cudaEvent_t ev = nullptr;
+    std::shared_ptr<char> host;    // pinned: upload image, then [heads | places]
+    size_t up_bytes = 0, heads_bytes = 0, places_bytes = 0;
+    double t0 = 0;
+};
+
+struct ServeEngine {
+    plp_handle* h;
+    int device = 0, sms = 148;
+    std::shared_ptr<HostPool> pool;
+    // device
+    char* arena = nullptr;
+    size_t cap = 0;
+    int* ctl = nullptr;            // [0] head, [1] tail, [2] stop, [3] error flag, [4] abort
+    int2* ring = nullptr;
+    // host
+    long long* m_done_seq = nullptr;   // host-mapped completion records
+    int2* m_done_best = nullptr;
+    int* h_word = nullptr;         // pinned: [0] head after a launch, [1 ..] tail values to copy
+    ServeArgs args{};
+    cudaStream_t up = nullptr, kern = nullptr, down = nullptr;
+    cudaEvent_t ev_kern = nullptr, ev_go = nullptr;
+    bool running = false, broken = false, stop_sent = false;
+    ServeConfig cfg;
+    const uint32_t* mt_init = nullptr;
+    struct LiveRegion {
+        size_t off, end;
+        bool freed;
+    };
+    std::deque<LiveRegion> live;       // arena regions in allocation order
+    long long live_base = 0;           // region id of live.front()
+    size_t alloc_pos = 0;
+    std::deque<ServeJob*> pending;     // submitted, not yet taken by the engine (h->mu)
+    std::deque<ServeJob*> fresh;       // taken, not yet admitted (engine thread)
+    std::deque<ServeJob*> active;      // admitted (engine thread)
+    std::condition_variable cv;        // new pending requests (h->mu)
+    long long next_seq = 1;
+    long long published = 0, restarts_done = 0;
+    int tail = 0, tail_copies = 0;
+    std::atomic<long long> n_launches{0}, n_served{0}, n_fallbacks{0}, n_waved{0};
+    bool quit = false;                 // h->mu
+    double last_busy = 0;
+    std::thread th;
+    Pinned pin;                        // the fallback's staging
+
+    explicit ServeEngine(plp_handle* hh) : h(hh) {}
+
+    static bool eligible(const plp_run_opts& o) {
+        return o.engine == 0 && o.passes == 1 && o.time_limit_s < 0 && !o.best_only;
+    }
+
+    int init(size_t arena_bytes) {
+        device = h->device;
+        sms = h->sms;
+        pool = h->pool;
+        cudaError_t e = cudaSetDevice(device);
+        if (e != cudaSuccess) return set_cuda_error("serving engine device", e);
+        int status = PLP_OK;
+        mt_init = device_mt_init(&status);
+        if (!mt_init) return status;
+        cap = arena_bytes;
+        e = cudaMalloc(&arena, cap);
+        if (e == cudaSuccess) e = cudaMalloc(&ctl, 64);
+        if (e == cudaSuccess) e = cudaMemset(ctl, 0, 64);
+        if (e == cudaSuccess) e = cudaMalloc(&ring, sizeof(int2) * SERVE_RING);
+        if (e == cudaSuccess)
+            e = cudaHostAlloc(&m_done_seq, sizeof(long long) * SERVE_RECORDS, cudaHostAllocMapped);
+        if (e == cudaSuccess) e = cudaHostAlloc(&m_done_best, sizeof(int2) * SERVE_RECORDS, cudaHostAllocMapped);
+        if (e == cudaSuccess) e = cudaMallocHost(&h_word, sizeof(int) * (1 + SERVE_RECORDS));
+        for (cudaStream_t* s : {&up, &kern, &down})
+            if (e == cudaSuccess) e = cudaStreamCreateWithFlags(s, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev_kern, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev_go, cudaEventDisableTiming);
+        void* p = nullptr;
+        if (e == cudaSuccess) {
+            for (int i = 0; i < SERVE_RECORDS; i++) m_done_seq[i] = -1;
+            std::memset(m_done_best, 0, sizeof(int2) * SERVE_RECORDS);
+            h_word[0] = 0;
+            e = cudaHostGetDevicePointer(&p, m_done_seq, 0);
+        }
+        args.done_seq = static_cast<volatile long long*>(p);
+        if (e == cudaSuccess) e = cudaHostGetDevicePointer(&p, m_done_best, 0);
+        args.done_best = static_cast<int2*>(p);
+        if (e != cudaSuccess) return set_cuda_error("serving engine set-up", e);
+        args.head = ctl;
+        args.tail = ctl + 1;
+        args.stop = ctl + 2;
+        args.ring = ring;
+        args.ring_mask = SERVE_RING - 1;
+        args.idle_polls = SERVE_IDLE_POLLS;
+        cfg.P = std::max(h->tile.P, 256);
+        cfg.C = std::max(h->tile.C, 768);
+        th = std::thread([this] { loop(); });
+        return PLP_OK;
+    }
+
+    ~ServeEngine() {
+        {
+            std::lock_guard<std::mutex> lk(h->mu);
+            quit = true;
+        }
+        cv.notify_all();
+        if (th.joinable()) th.join();
+        cudaSetDevice(device);
+        if (running) {
+            send_stop(1);
+            cudaEventSynchronize(ev_kern);   // decoders finish their items and leave
+        }
+        for (cudaStream_t s : {up, kern, down})
+            if (s) cudaStreamSynchronize(s);
+        for (ServeJob* j : active) {
+            if (j->ev) cudaEventDestroy(j->ev);
+            delete j;
+        }
+        for (ServeJob* j : fresh) delete j;
+        for (ServeJob* j : pending) delete j;
+        for (cudaStream_t s : {up, kern, down})
+            if (s) cudaStreamDestroy(s);
+        for (cudaEvent_t v : {ev_kern, ev_go})
+            if (v) cudaEventDestroy(v);
+        for (void* q : {(void*)m_done_seq, (void*)m_done_best, (void*)h_word})
+            if (q) cudaFreeHost(q);
+        for (void* q : {(void*)arena, (void*)ctl, (void*)ring})
+            if (q) cudaFree(q);
+    }
+
+    // the stop word, in stream order on the upload stream
+    void send_stop(int v) {
+        cudaMemsetAsync(ctl + 2, v ? 1 : 0, sizeof(int), up);
+        stop_sent = v != 0;
+    }
+
+    bool allocate(ServeJob& j) {
+        if (live.empty()) {
+            alloc_pos = 0;
+            if (!serve_layout(j.b, 0, cap, j.g)) return false;
+        } else {
+            const size_t oldest = live.front().off;
+            if (alloc_pos >= oldest) {         // free: [alloc_pos, cap) and [0, oldest)
+                if (!serve_layout(j.b, alloc_pos, cap, j.g) && !serve_layout(j.b, 0, oldest, j.g)) return false;
+            } else if (!serve_layout(j.b, alloc_pos, oldest, j.g)) {
+                return false;
+            }
+        }
+        alloc_pos = j.g.end;
+        live.push_back({j.g.off, j.g.end, false});
+        j.region = live_base + (long long)live.size() - 1;
+        return true;
+    }
+
+    void release(ServeJob& j) {
+        live[(size_t)(j.region - live_base)].freed = true;
+        while (!live.empty() && live.front().freed) {
+            live.pop_front();
+            live_base++;
+        }
+    }
+
+    void unallocate(ServeJob& j) {     // the newest region only
+        if (!live.empty() && j.region == live_base + (long long)live.size() - 1) {
+            live.pop_back();
+            alloc_pos = live.empty() ? 0 : live.back().end;
+        }
+    }
+
+    bool compatible(const Batch& b) const {
+        if (!cfg.valid) return true;
+        if (cfg.sup16 && !b.sup16_ok) return false;
+        if (cfg.Hz == 0) return true;
+        return b.Hz != 0 && b.Hz <= cfg.Hz;
+    }
+
+    void merge_config(const Batch& b) {
+        if (!cfg.valid) {
+            cfg.Hz = b.Hz;
+            cfg.sup16 = b.sup16_ok;
+            cfg.valid = true;
+            return;
+        }
+        cfg.Hz = (cfg.Hz == 0 || b.Hz == 0) ? 0 : std::max(cfg.Hz, b.Hz);
+        cfg.sup16 = cfg.sup16 && b.sup16_ok;
+    }
+
+    void complete(ServeJob& j, int status, plp_result* res, const std::string& err) {
+        {
+            std::lock_guard<std::mutex> lk(h->mu);
+            Request* r = j.r;
+            r->running = false;
+            r->t_done = now_seconds();
+            if (status == PLP_OK) {
+                r->result = res;
+                r->status = r->cancelled ? PLP_E_CANCELLED : PLP_OK;
+                if (r->cancelled) r->err = "request was cancelled";
+            } else {
+                r->status = status;
+                r->err = err;
+            }
+        }
+        h->cv.notify_all();
+    }
+
+    cudaError_t launch() {
+        DecodeLaunch L{};
+        L.inst = reinterpret_cast<const InstDesc*>(arena);
+        L.step_type = reinterpret_cast<const int*>(arena);
+        L.types = reinterpret_cast<const TypeOrs*>(arena);
+        L.heads = reinterpret_cast<SlotHead*>(arena);
+        L.places = reinterpret_cast<unsigned long long*>(arena);
+        L.err_flag = ctl + 3;
+        L.abort = ctl + 4;
+        L.mt_init = mt_init;
+        L.P = cfg.P;
+        L.C = cfg.C;
+        L.Hz = cfg.Hz;
+        L.sup16 = cfg.sup16;
+        L.engine = 0;
+        L.warps_per_decoder = 1;
+        L.decoders_per_cta = cfg.D;
+        L.min_blocks = cfg.M;
+        int occ = 0;
+        cudaError_t e = serve_occupancy(cfg.P, cfg.C, cfg.Hz, cfg.D, cfg.M, cfg.sup16, &occ);
+        if (e != cudaSuccess) return e;
+        if (occ < 1) return cudaErrorInvalidConfiguration;
+        L.ctas = sms * occ;
+        send_stop(0);
+        e = cudaEventRecord(ev_go, up);                 // the launch follows every upload so far
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(kern, ev_go, 0);
+        if (e == cudaSuccess) e = launch_serve(L, args, kern);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(h_word, ctl, sizeof(int), cudaMemcpyDeviceToHost, kern);
+        if (e == cudaSuccess) e = cudaEventRecord(ev_kern, kern);
+        if (e == cudaSuccess) {
+            running = true;
+            n_launches++;
+        }
+        return e;
+    }
+
+    // tables, work items and the new tail of an admitted request, in one
+    // stream pass on the upload stream
+    int publish(ServeJob& j) {
+        const InstDesc& d0 = j.b.desc[0];
+        const int R = d0.restarts;
+        const size_t tab = j.g.heads - j.g.desc;
+        j.up_bytes = tab + (size_t)R * sizeof(int2);
+        j.heads_bytes = (size_t)R * sizeof(SlotHead);
+        j.places_bytes = (size_t)R * d0.place_stride * 8;
+        j.host = pool_take(pool, std::max(j.up_bytes, j.heads_bytes + j.places_bytes));
+        if (!j.host) return set_error(PLP_E_CAPACITY, "serving: no pinned host memory for a request");
+        char* img = j.host.get();
+        std::memset(img, 0, tab);
+        InstDesc d = d0;
+        d.step_off = (int)(j.g.steps / sizeof(int));
+        d.type_off = (int)(j.g.types / sizeof(TypeOrs));
+        d.slot_base = (int)(j.g.heads / sizeof(SlotHead));
+        d.place_off = (long long)(j.g.places / 8);
+        std::memcpy(img, &d, sizeof d);
+        ServeTail tl{};
+        tl.done_slot = j.slot;
+        tl.seq = j.seq;
+        std::memcpy(img + sizeof(InstDesc), &tl, sizeof tl);
+        std::memcpy(img + (j.g.steps - j.g.desc), j.b.steps.data(), j.b.steps.size() * sizeof(int));
+        std::memcpy(img + (j.g.types - j.g.desc), j.b.types.data(), j.b.types.size() * sizeof(TypeOrs));
+        int2* items = reinterpret_cast<int2*>(img + tab);
+        const int di = (int)(j.g.desc / sizeof(InstDesc));
+        for (int k = 0; k < R; k++) items[k] = make_int2(di, k);
+        cudaError_t e = cudaMemcpyAsync(arena + j.g.desc, img, tab, cudaMemcpyHostToDevice, up);
+        const int pos = tail & (SERVE_RING - 1);
+        const int first = std::min(R, SERVE_RING - pos);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(ring + pos, items, first * sizeof(int2), cudaMemcpyHostToDevice, up);
+        if (e == cudaSuccess && first < R)
+            e = cudaMemcpyAsync(ring, items + first, (R - first) * sizeof(int2), cudaMemcpyHostToDevice, up);
+        tail += R;
+        int* src = h_word + 1 + (tail_copies++ % SERVE_RECORDS);
+        *src = tail;
+        if (e == cudaSuccess) e = cudaMemcpyAsync(ctl + 1, src, sizeof(int), cudaMemcpyHostToDevice, up);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&j.ev, cudaEventDisableTiming);
+        if (e != cudaSuccess) return set_cuda_error("serving upload", e);
+        published += R;
+        return PLP_OK;
+    }
+
+    // the wave path's code, for a request whose restarts outgrew the serving tile
+    void fallback(ServeJob& j) {
+        if (running) {                 // the serving launch holds the SMs: let it finish its items
+            send_stop(1);
+            cudaEventSynchronize(ev_kern);
+            running = false;
+        }
+        TileConfig tile;
+        {
+            std::lock_guard<std::mutex> lk(h->mu);
+            tile = h->tile;
+        }
+        Batch b;
+        const double t0 = now_seconds();
+        int s = b.build({&j.inst}, {j.opts});
+        if (s == PLP_OK) s = run_batch(b, down, pin, sms, tile, &pool);
+        std::vector<plp_result*> res;
+        if (s == PLP_OK) res = collect(b, now_seconds() - t0);
+        complete(j, s, s == PLP_OK ? res[0] : nullptr, s == PLP_OK ? "" : g_err);
+    }
+
+    plp_result* result_of(ServeJob& j) {
+        const InstDesc& d = j.b.desc[0];
+        auto* r = new plp_result;
+        r->restarts = d.restarts;
+        r->stride = d.place_stride;
+        r->ors = j.b.inst_ors[0];
+        r->L = d.L; r->W = d.W; r->H = d.H;
+        r->steps = j.b.steps;
+        r->block = j.host;
+        r->heads = reinterpret_cast<const SlotHead*>(j.host.get());
+        r->seed0 = d.seed;
+        r->time_s = now_seconds() - j.t0;
+        const int2 best = m_done_best[j.slot];
+        r->best = best.x;
+        r->best_fallback = best.y;
+        r->kept_all = true;
+        r->packed = reinterpret_cast<const unsigned long long*>(j.host.get() + j.heads_bytes);
+        return r;
+    }
+
+    void route_to_waves(ServeJob* j) {
+        n_waved++;
+        {
+            std::lock_guard<std::mutex> lk(h->mu);
+            h->queue.push_back(j->id);
+        }
+        h->cv_sched.notify_all();
+        delete j;
+    }
+
+    void fail_all(const std::string& why) {
+        broken = true;
+        for (ServeJob* j : active) {
+            complete(*j, PLP_E_CUDA, nullptr, why);
+            if (j->ev) cudaEventDestroy(j->ev);
+            delete j;
+        }
+        active.clear();
+        live.clear();
+        live_base = 0;
+        alloc_pos = 0;
+        for (ServeJob* j : fresh) route_to_waves(j);
+        fresh.clear();
+    }
+
+    // admission, in arrival order; true when a request moved
+    bool admit() {
+        bool progress = false;
+        while (!fresh.empty()) {
+            ServeJob* j = fresh.front();
+            bool gone = false;
+            {
+                // plp_cancel marks a request cancelled before admission itself
+                std::lock_guard<std::mutex> lk(h->mu);
+                auto it = h->reqs.find(j->id);
+                gone = it == h->reqs.end() || it->second->status != PLP_E_PENDING || it->second->cancelled;
+            }
+            if (gone) {
+                fresh.pop_front();
+                h->cv.notify_all();
+                delete j;
+                progress = true;
+                continue;
+            }
+            if (broken) {
+                fresh.pop_front();
+                route_to_waves(j);
+                progress = true;
+                continue;
+            }
+            if (!j->built) {
+                const int s = j->b.build({&j->inst}, {j->opts});
+                j->built = true;
+                ServeRegion whole;
+                if (s != PLP_OK || !serve_layout(j->b, 0, cap, whole) || j->b.desc[0].restarts > SERVE_RING / 4) {
+                    fresh.pop_front();               // errors and oversized requests: the wave path
+                    route_to_waves(j);
+                    progress = true;
+                    continue;
+                }
+            }
+            if (!compatible(j->b)) {
+                if (!active.empty()) break;            // drain first
+                if (running) {
+                    if (!stop_sent) send_stop(1);
+                    break;
+                }
+                cfg.valid = false;                     // the next launch takes the merged configuration
+            }
+            if (active.size() >= SERVE_RECORDS / 2 ||
+                published - restarts_done + j->b.desc[0].restarts > SERVE_RING / 2 || !allocate(*j))
+                break;                                 // wait for requests to finish
+            j->t0 = now_seconds();
+            {
+                std::lock_guard<std::mutex> lk(h->mu);
+                auto it = h->reqs.find(j->id);
+                if (it == h->reqs.end() || it->second->status != PLP_E_PENDING || it->second->cancelled) {
+                    gone = true;
+                } else {
+                    j->r = it->second.get();
+                    j->r->running = true;
+                    j->r->t_start = j->t0;
+                }
+            }
+            fresh.pop_front();
+            if (gone) {                                // cancelled meanwhile: give the region back
+                unallocate(*j);
+                delete j;
+                progress = true;
+                continue;
+            }
+            merge_config(j->b);
+            j->seq = next_seq++;
+            j->slot = (int)(j->seq % SERVE_RECORDS);
+            const int s = publish(*j);
+            if (s != PLP_OK) {
+                unallocate(*j);
+                complete(*j, s, nullptr, g_err);
+                delete j;
+                progress = true;
+                continue;
+            }
+            j->state = 1;
+            active.push_back(j);
+            progress = true;
+        }
+        return progress;
+    }
+
+    // one pass of the scheduler; true when something changed
+    bool step() {
+        bool progress = admit();
+        // the launch: started again whenever published work is unclaimed
+        if (running && cudaEventQuery(ev_kern) == cudaSuccess) {
+            running = false;
+            progress = true;
+        }
+        if (!running && !broken && *reinterpret_cast<volatile int*>(h_word) < tail) {
+            const cudaError_t e = launch();
+            if (e != cudaSuccess) {
+                cudaGetLastError();
+                fail_all(std::string("serving launch failed: ") + cudaGetErrorString(e));
+                return true;
+            }
+            progress = true;
+        }
+        // completions: copy out the results of finished requests
+        for (ServeJob* j : active) {
+            if (j->state != 1) continue;
+            if (__atomic_load_n(&m_done_seq[j->slot], __ATOMIC_ACQUIRE) != j->seq) continue;
+            cudaError_t e = cudaMemcpyAsync(j->host.get(), arena + j->g.heads, j->heads_bytes,
+                                            cudaMemcpyDeviceToHost, down);
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(j->host.get() + j->heads_bytes, arena + j->g.places, j->places_bytes,
+                                    cudaMemcpyDeviceToHost, down);
+            if (e == cudaSuccess) e = cudaEventRecord(j->ev, down);
+            if (e != cudaSuccess) {
+                cudaGetLastError();
+                fail_all("serving result copy failed");
+                return true;
+            }
+            restarts_done += j->b.desc[0].restarts;
+            j->state = 2;
+            progress = true;
+        }
+        for (auto it = active.begin(); it != active.end();) {
+            ServeJob* j = *it;
+            if (j->state != 2 || cudaEventQuery(j->ev) != cudaSuccess) {
+                ++it;
+                continue;
+            }
+            const SlotHead* hd = reinterpret_cast<const SlotHead*>(j->host.get());
+            bool overflow = false;
+            for (int k = 0; k < j->b.desc[0].restarts; k++) overflow = overflow || hd[k].err != ERR_NONE;
+            release(*j);
+            cudaEventDestroy(j->ev);
+            j->ev = nullptr;
+            if (overflow) {
+                n_fallbacks++;
+                fallback(*j);
+            } else {
+                n_served++;
+                complete(*j, PLP_OK, result_of(*j), "");
+            }
+            delete j;
+            it = active.erase(it);
+            progress = true;
+        }
+        // idle: stop the launch; with nothing in flight the counters restart at 0
+        const double now = now_seconds();
+        if (progress || !active.empty() || !fresh.empty()) last_busy = now;
+        if (running && !stop_sent && active.empty() && fresh.empty() && now - last_busy > SERVE_IDLE_STOP_S)
+            send_stop(1);
+        if (!running && active.empty() && fresh.empty() && tail > (1 << 30)) {
+            cudaMemsetAsync(ctl, 0, 2 * sizeof(int), up);
+            cudaStreamSynchronize(up);
+            tail = 0;
+            h_word[0] = 0;
+        }
+        return progress;
+    }
+
+    void loop() {
+        cudaSetDevice(device);
+        for (;;) {
+            {
+                std::unique_lock<std::mutex> lk(h->mu);
+                if (quit) break;
+                if (active.empty() && fresh.empty() && pending.empty() && !running)
+                    cv.wait_for(lk, std::chrono::milliseconds(50), [&] { return quit || !pending.empty(); });
+                if (quit) break;
+                while (!pending.empty()) {
+                    fresh.push_back(pending.front());
+                    pending.pop_front();
+                }
+            }
+            if (!step()) {
+                if (active.empty() && fresh.empty()) std::this_thread::sleep_for(std::chrono::microseconds(200));
+                else std::this_thread::yield();
+            }
+        }
+    }
+};
+
+// The handle's serving engine, made on first use. Its arena is half the
+// budget, at most PLP_SERVE_ARENA_MB (default 4096 MiB), reserved from the
+// budget that the wave path admits by. Null when serving is off (PLP_SERVE=0)
+// or could not be set up; eligible requests then take the wave path.
+ServeEngine* serve_engine(plp_handle* h) {
+    std::lock_guard<std::mutex> g(h->serve_mu);
+    if (h->serve || h->serve_off) return h->serve;
+    const char* v = std::getenv("PLP_SERVE");
+    if (v && std::string(v) == "0") {
+        h->serve_off = true;
+        return nullptr;
+    }
+    size_t arena = (size_t)4096 << 20;
+    if (const char* a = std::getenv("PLP_SERVE_ARENA_MB")) {
+        char* end = nullptr;
+        const unsigned long long mb = std::strtoull(a, &end, 10);
+        if (end != a && mb > 0) arena = (size_t)mb << 20;
+    }
+    arena = std::min(arena, h->budget / 2);
+    if (arena < ((size_t)1 << 16)) {
+        h->serve_off = true;
+        return nullptr;
+    }
+    {
+        std::lock_guard<std::mutex> lk(h->mu);
+        if (h->in_use + arena > h->budget) {
+            h->serve_off = true;
+            return nullptr;
+        }
+        h->in_use += arena;
+    }
+    auto* eng = new ServeEngine(h);
+    if (eng->init(arena) != PLP_OK) {
+        cudaGetLastError();
+        delete eng;
+        std::lock_guard<std::mutex> lk(h->mu);
+        h->in_use -= arena;
+        h->serve_off = true;
+        return nullptr;
+    }
+    h->serve = eng;
+    return eng;
 }
 
 }  // namespace
@@ -1673,10 +2328,24 @@ void plp_destroy(plp_handle* h) {
     }
     h->cv_sched.notify_all();
     for (auto& t : h->workers) t.join();
+    delete h->serve;              // stops its launch and thread
+    h->serve = nullptr;
     for (auto& kv : h->reqs) delete kv.second->result;
     for (auto s : h->streams) cudaStreamDestroy(s);
     if (h->sync_stream) cudaStreamDestroy(h->sync_stream);
     delete h;
+}
+
+int plp_serve_counters(plp_handle* h, int64_t* launches, int64_t* served, int64_t* fallbacks,
+                       int64_t* waved) {
+    if (!h) return set_error(PLP_E_INVALID, "plp_serve_counters: null handle");
+    std::lock_guard<std::mutex> g(h->serve_mu);
+    const ServeEngine* e = h->serve;
+    if (launches) *launches = e ? e->n_launches.load() : 0;
+    if (served) *served = e ? e->n_served.load() : 0;
+    if (fallbacks) *fallbacks = e ? e->n_fallbacks.load() : 0;
+    if (waved) *waved = e ? e->n_waved.load() : 0;
+    return PLP_OK;
 }
 
 int plp_debug_sync_bound(plp_handle* h, int32_t wait_limit, int32_t skip_warp) {
@@ -1888,14 +2557,27 @@ int plp_submit(plp_handle* h, const plp_instance* inst, const plp_run_opts* opts
         return s;
     }
     r->t_submit = now_seconds();
+    ServeEngine* eng = ServeEngine::eligible(*opts) ? serve_engine(h) : nullptr;
+    ServeJob* job = nullptr;
+    if (eng) {
+        job = new ServeJob;
+        job->inst = inst->inst;
+        job->opts = *opts;
+    }
     {
         std::lock_guard<std::mutex> lk(h->mu);
         r->id = h->next_id++;
         *id = r->id;
-        h->queue.push_back(r->id);
+        if (job) {
+            job->id = r->id;
+            eng->pending.push_back(job);
+        } else {
+            h->queue.push_back(r->id);
+        }
         h->reqs[r->id] = std::move(r);
     }
-    h->cv_sched.notify_one();
+    if (job) eng->cv.notify_one();
+    else h->cv_sched.notify_one();
     return PLP_OK;
 }
 

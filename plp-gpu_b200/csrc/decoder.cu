@@ -1183,8 +1183,125 @@ __device__ __forceinline__ int place1(int t, int pp, bool full, uint32_t* mt, in
     return ERR_NONE;
 }
 
-template <typename SupT>
-__device__ __forceinline__ void decoder1_body(const DecoderArgs& a, unsigned char* base, int gdec) {
+// ---------------------------------------------------------------------------
+// serving: work from a host-published ring, completion on the device
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int ld_acquire_gpu(const int* p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ int2 ld_relaxed_gpu_int2(const int2* p) {
+    int x, y;
+    asm volatile("ld.relaxed.gpu.global.v2.s32 {%0, %1}, [%2];" : "=r"(x), "=r"(y) : "l"(p) : "memory");
+    return make_int2(x, y);
+}
+
+__device__ __forceinline__ void st_release_sys(volatile long long* p, long long v) {
+    asm volatile("st.release.sys.b64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// Lane 0: claims the next published work item, or returns -1 once the host
+// has asked the launch to stop (and nothing is left) or after idle_polls
+// empty polls. The host publishes by stream-ordered copies into device
+// memory (items first, then the tail), so the polls stay on this GPU's L2.
+// Every loop is bounded: the inner one by the items published, the outer
+// one by idle_polls.
+__device__ __forceinline__ int serve_claim(const ServeArgs& s) {
+    unsigned ns = 32;
+    for (int k = 0; k < s.idle_polls; k++) {
+        const int t = ld_acquire_gpu(s.tail);
+        int h = *reinterpret_cast<volatile int*>(s.head);
+        while (h < t) {
+            const int prev = atomicCAS(s.head, h, h + 1);
+            if (prev == h) return h;
+            h = prev;
+        }
+        if (ld_acquire_gpu(s.stop)) return -1;
+        __nanosleep(ns);
+        if (ns < 4096) ns <<= 1;
+    }
+    return -1;
+}
+
+// A request descriptor read through L2 (serving arenas reuse addresses while
+// the launch runs, so no table may come from a stale L1 line).
+__device__ __forceinline__ InstDesc load_desc_cg(const InstDesc* p) {
+    static_assert(sizeof(InstDesc) % 8 == 0, "InstDesc is copied in 8-byte words");
+    InstDesc d;
+    const long long* src = reinterpret_cast<const long long*>(p);
+    long long* dst = reinterpret_cast<long long*>(&d);
+#pragma unroll
+    for (int i = 0; i < (int)(sizeof(InstDesc) / 8); i++) dst[i] = __ldcg(src + i);
+    return d;
+}
+
+template <bool CG>
+__device__ __forceinline__ int ld_table(const int* p) { return CG ? __ldcg(p) : *p; }
+
+// Best restart of one instance, one warp: accepted first, then max (volume,
+// n_boxes), the earliest restart on ties (the strict > of
+// gpu/plp_common.hpp:507-511). CG: the heads are read through L2.
+template <bool CG>
+__device__ __forceinline__ int2 select_best_warp(const InstDesc& I, const SlotHead* heads, int lane) {
+    int br = -1, bacc = 0, bn = 0;
+    long long bv = -1;
+    for (int r = lane; r < I.restarts; r += 32) {
+        const SlotHead* hp = heads + I.slot_base + r;
+        const int fb = CG ? __ldcg(&hp->fallback) : hp->fallback;
+        const long long vol = CG ? __ldcg(&hp->volume) : hp->volume;
+        const int nbx = CG ? __ldcg(&hp->n_boxes) : hp->n_boxes;
+        const int acc = fb ? 0 : 1;
+        const bool better = br < 0 || acc > bacc || (acc == bacc && (vol > bv || (vol == bv && nbx > bn)));
+        if (better) { br = r; bacc = acc; bv = vol; bn = nbx; }
+    }
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) {
+        const int r2 = __shfl_down_sync(FULL, br, d);
+        const int a2 = __shfl_down_sync(FULL, bacc, d);
+        const long long v2 = __shfl_down_sync(FULL, bv, d);
+        const int n2 = __shfl_down_sync(FULL, bn, d);
+        bool better;
+        if (r2 < 0) better = false;
+        else if (br < 0) better = true;
+        else if (a2 != bacc) better = a2 > bacc;
+        else if (v2 != bv) better = v2 > bv;
+        else if (n2 != bn) better = n2 > bn;
+        else better = r2 < br;
+        if (better) { br = r2; bacc = a2; bv = v2; bn = n2; }
+    }
+    return make_int2(__shfl_sync(FULL, br, 0), __shfl_sync(FULL, bacc, 0) ? 0 : 1);
+}
+
+// After a restart's head is written: the warp that finishes the request's
+// last restart selects its best restart and publishes it, with the request's
+// sequence number, in the host-mapped completion record.
+__device__ __forceinline__ void serve_finish(const DecoderArgs& a, const ServeArgs& s, int di, const InstDesc& I,
+                                             int lane) {
+    ServeTail* tl = reinterpret_cast<ServeTail*>(const_cast<InstDesc*>(a.inst) + di + 1);
+    int last = 0;
+    if (lane == 0) {
+        __threadfence();
+        last = atomicAdd(&tl->done_count, 1) == I.restarts - 1;
+    }
+    last = __shfl_sync(FULL, last, 0);
+    if (!last) return;
+    __threadfence();
+    const int2 b = select_best_warp<true>(I, a.heads, lane);
+    if (lane == 0) {
+        const int slot = __ldcg(&tl->done_slot);
+        const long long seq = __ldcg(&tl->seq);
+        s.done_best[slot] = b;
+        __threadfence_system();
+        st_release_sys(s.done_seq + slot, seq);
+    }
+    __syncwarp();
+}
+
+template <typename SupT, bool SERVE>
+__device__ __forceinline__ void decoder1_body(const DecoderArgs& a, unsigned char* base, int gdec,
+                                              const ServeArgs& sv) {
     const int lane = threadIdx.x & 31;
     const Dec1Layout lay = dec1_layout(a.P, a.C, a.Hz, (int)sizeof(SupT));
     const int C = a.C;
@@ -1200,15 +1317,30 @@ __device__ __forceinline__ void decoder1_body(const DecoderArgs& a, unsigned cha
     unsigned short* wi = reinterpret_cast<unsigned short*>(base + lay.off_wi);
     unsigned short* zt = a.Hz ? reinterpret_cast<unsigned short*>(base + lay.off_zt) : nullptr;
 
-    const int n_work = a.n_work_dev ? *a.n_work_dev : a.n_work;
+    const int n_work = SERVE ? 0 : (a.n_work_dev ? *a.n_work_dev : a.n_work);
     for (;;) {
         if (*reinterpret_cast<volatile int*>(a.abort)) return;
-        int item = 0;
-        if (lane == 0) item = atomicAdd(a.work_next, 1);
-        item = __shfl_sync(FULL, item, 0);
-        if (item >= n_work) break;
-        const int2 wk = a.work[item];
-        const InstDesc I = a.inst[wk.x];
+        int2 wk;
+        if (SERVE) {
+            int item = -1, wx = 0, wy = 0;
+            if (lane == 0) {
+                item = serve_claim(sv);
+                if (item >= 0) {
+                    const int2 w = ld_relaxed_gpu_int2(sv.ring + (item & sv.ring_mask));
+                    wx = w.x;
+                    wy = w.y;
+                }
+            }
+            if (__shfl_sync(FULL, item, 0) < 0) break;
+            wk = make_int2(__shfl_sync(FULL, wx, 0), __shfl_sync(FULL, wy, 0));
+        } else {
+            int item = 0;
+            if (lane == 0) item = atomicAdd(a.work_next, 1);
+            item = __shfl_sync(FULL, item, 0);
+            if (item >= n_work) break;
+            wk = a.work[item];
+        }
+        const InstDesc I = SERVE ? load_desc_cg(a.inst + wk.x) : a.inst[wk.x];
         const int restart = wk.y;
         const int slot = I.slot_base + restart;
         const int L = I.L, W = I.W, H = I.H;
@@ -1245,20 +1377,20 @@ __device__ __forceinline__ void decoder1_body(const DecoderArgs& a, unsigned cha
             bool pending = false;   // a placed box not yet applied to the valid states
             int4 B = make_int4(0, 0, 0, 0);
             int Bz = 0, Bz2 = 0;
-            int t_next = I.n_steps > 0 ? a.step_type[I.step_off] : 0;
+            int t_next = I.n_steps > 0 ? ld_table<SERVE>(a.step_type + I.step_off) : 0;
             for (int sti = 0; sti < I.n_steps; sti++) {
                 const int t = t_next;
-                if (sti + 1 < I.n_steps) t_next = a.step_type[I.step_off + sti + 1];
+                if (sti + 1 < I.n_steps) t_next = ld_table<SERVE>(a.step_type + I.step_off + sti + 1);
                 const TypeOrs& T = a.types[I.type_off + t];
                 StepOrs S;
-                S.no = T.n;
+                S.no = ld_table<SERVE>(&T.n);
                 if (S.no == 0) continue;
                 S.wmax = S.dmax = S.hmax = 0;
 #pragma unroll
                 for (int o = 0; o < 6; o++) {
-                    S.ow[o] = T.w[o];
-                    S.od[o] = T.d[o];
-                    S.oh[o] = T.h[o];
+                    S.ow[o] = ld_table<SERVE>(&T.w[o]);
+                    S.od[o] = ld_table<SERVE>(&T.d[o]);
+                    S.oh[o] = ld_table<SERVE>(&T.h[o]);
                     S.wd[o] = S.ow[o] * S.od[o];
                     S.wmax = max(S.wmax, S.ow[o]);
                     S.dmax = max(S.dmax, S.od[o]);
@@ -1380,6 +1512,7 @@ __device__ __forceinline__ void decoder1_body(const DecoderArgs& a, unsigned cha
             a.heads[slot] = h;
         }
         __syncwarp();
+        if (SERVE) serve_finish(a, sv, wk.x, I, lane);
     }
 }
 
@@ -1390,7 +1523,17 @@ __global__ void __launch_bounds__(32 * D, M) decoder1_kernel(DecoderArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int dec = threadIdx.x >> 5;
     const Dec1Layout lay = dec1_layout(a.P, a.C, a.Hz, (int)sizeof(SupT));
-    decoder1_body<SupT>(a, smem_raw + (size_t)dec * lay.bytes, blockIdx.x * D + dec);
+    decoder1_body<SupT, false>(a, smem_raw + (size_t)dec * lay.bytes, blockIdx.x * D + dec, ServeArgs{});
+}
+
+// The serving launch: the single-warp decoder over the host-published ring.
+template <int D, int M, int S16>
+__global__ void __launch_bounds__(32 * D, M) serve_kernel(DecoderArgs a, ServeArgs s) {
+    using SupT = typename std::conditional<S16 != 0, unsigned short, int>::type;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int dec = threadIdx.x >> 5;
+    const Dec1Layout lay = dec1_layout(a.P, a.C, a.Hz, (int)sizeof(SupT));
+    decoder1_body<SupT, true>(a, smem_raw + (size_t)dec * lay.bytes, blockIdx.x * D + dec, s);
 }
 
 // ---------------------------------------------------------------------------
@@ -1403,32 +1546,8 @@ __global__ void select_best_kernel(const InstDesc* __restrict__ inst, int n_inst
     const int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (i >= n_inst) return;
     const InstDesc I = inst[i];
-    // key: accepted, volume, n_boxes, then the smallest restart wins
-    int br = -1, bacc = 0, bn = 0;
-    long long bv = -1;
-    for (int r = lane; r < I.restarts; r += 32) {
-        const SlotHead h = heads[I.slot_base + r];
-        const int acc = h.fallback ? 0 : 1;
-        const bool better = br < 0 || acc > bacc ||
-                            (acc == bacc && (h.volume > bv || (h.volume == bv && h.n_boxes > bn)));
-        if (better) { br = r; bacc = acc; bv = h.volume; bn = h.n_boxes; }
-    }
-#pragma unroll
-    for (int d = 16; d > 0; d >>= 1) {
-        const int r2 = __shfl_down_sync(FULL, br, d);
-        const int a2 = __shfl_down_sync(FULL, bacc, d);
-        const long long v2 = __shfl_down_sync(FULL, bv, d);
-        const int n2 = __shfl_down_sync(FULL, bn, d);
-        bool better;
-        if (r2 < 0) better = false;
-        else if (br < 0) better = true;
-        else if (a2 != bacc) better = a2 > bacc;
-        else if (v2 != bv) better = v2 > bv;
-        else if (n2 != bn) better = n2 > bn;
-        else better = r2 < br;
-        if (better) { br = r2; bacc = a2; bv = v2; bn = n2; }
-    }
-    if (lane == 0) best[i] = make_int2(br, bacc ? 0 : 1);
+    const int2 b = select_best_warp<false>(I, heads, lane);
+    if (lane == 0) best[i] = b;
 }
 
 // ---------------------------------------------------------------------------
@@ -1689,6 +1808,41 @@ cudaError_t launch_decoder(const DecodeLaunch& L, cudaStream_t st) {
     cudaError_t e = configure_decoder(L);
     if (e != cudaSuccess) return e;
     return enqueue_decoder(L, st);
+}
+
+// ---- serving launches ------------------------------------------------------
+using ServeFn = void (*)(DecoderArgs, ServeArgs);
+#define PLP_SERVE_CONFIGS(X) X(1, 1) X(1, 12)
+
+static ServeFn serve_fn(int D, int M, int sup16) {
+#define PLP_PICK_SERVE(d, m) \
+    if (D == d && M == m) return sup16 ? serve_kernel<d, m, 1> : serve_kernel<d, m, 0>;
+    PLP_SERVE_CONFIGS(PLP_PICK_SERVE)
+#undef PLP_PICK_SERVE
+    return nullptr;
+}
+
+bool serve_config_supported(int D, int M) { return serve_fn(D, M, 0) != nullptr; }
+
+cudaError_t serve_occupancy(int P, int C, int Hz, int D, int M, int sup16, int* ctas_per_sm) {
+    ServeFn fn = serve_fn(D, M, sup16);
+    if (!fn) return cudaErrorInvalidConfiguration;
+    const int smem = decoder_smem_bytes(P, C, Hz, 1, sup16) * D;
+    cudaError_t e = ensure_dyn_smem(reinterpret_cast<const void*>(fn), smem);
+    if (e != cudaSuccess) return e;
+    return cached_occupancy(reinterpret_cast<const void*>(fn), 32 * D, smem, ctas_per_sm);
+}
+
+cudaError_t launch_serve(const DecodeLaunch& L, const ServeArgs& s, cudaStream_t st) {
+    ServeFn fn = serve_fn(L.decoders_per_cta, L.min_blocks, L.sup16);
+    if (!fn || L.warps_per_decoder != 1 || L.engine != 0) return cudaErrorInvalidConfiguration;
+    const int smem = decoder_smem_bytes(L.P, L.C, L.Hz, 1, L.sup16) * L.decoders_per_cta;
+    cudaError_t e = ensure_dyn_smem(reinterpret_cast<const void*>(fn), smem);
+    if (e != cudaSuccess) return e;
+    e = cudaMemsetAsync(L.abort, 0, sizeof(int), st);
+    if (e != cudaSuccess) return e;
+    fn<<<L.ctas, 32 * L.decoders_per_cta, smem, st>>>(decoder_args(L), s);
+    return cudaGetLastError();
 }
 
 cudaError_t decoder_occupancy(int P, int C, int Hz, int G, int D, int M, int* ctas_per_sm, int sup16) {

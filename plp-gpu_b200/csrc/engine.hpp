@@ -57,6 +57,34 @@ cudaError_t ensure_dyn_smem(const void* fn, int smem);
 cudaError_t cached_occupancy(const void* fn, int threads, int smem, int* ctas_per_sm);
 
 // work items whose restart overflowed its tile, appended to redo (count zeroed by the caller)
+// Serving: one persistent launch of the single-warp decoder takes its work
+// from a ring of (request descriptor, restart) items that the host publishes
+// while it runs, and the decoder that finishes a request's last restart
+// selects its best restart and reports it in host-mapped memory.
+//
+// A request's descriptor is followed in device memory by a ServeTail; the
+// launch's tables (descriptors, step types, orientations, slot heads,
+// placements) all live in one arena whose regions are reused while the
+// launch runs, so the serving kernel reads every table through L2.
+struct ServeTail {
+    int done_count;       // restarts finished (device atomics)
+    int done_slot;        // index of the request's host-mapped completion record
+    long long seq;        // the request's sequence number, written to that record
+};
+struct ServeArgs {
+    int* head;                      // device: work items claimed
+    const int* tail;                // device: work items published (written by stream-ordered copies)
+    const int* stop;                // device: nonzero = exit once no work is left
+    const int2* ring;               // device: work items (descriptor index, restart)
+    int ring_mask;                  // ring entries - 1 (a power of two)
+    volatile long long* done_seq;   // host-mapped: per completion record, the finished request's seq
+    int2* done_best;                // host-mapped: per completion record, (best restart, fallback)
+    int idle_polls;                 // empty polls before a decoder exits (about 4 us each)
+};
+bool serve_config_supported(int D, int M);
+cudaError_t serve_occupancy(int P, int C, int Hz, int D, int M, int sup16, int* ctas_per_sm);
+cudaError_t launch_serve(const DecodeLaunch& L, const ServeArgs& s, cudaStream_t st);
+
 cudaError_t launch_redo_collect(const int2* work, int n_work, const InstDesc* inst, const SlotHead* heads,
                                 int2* redo, int* count, int sms, cudaStream_t st);
 cudaError_t launch_select_best(const InstDesc* inst, int n_inst, const SlotHead* heads, int2* best,

@@ -108,6 +108,7 @@ def lib():
         "plp_destroy": (None, [P]),
         "plp_set_tile": (ctypes.c_int, [P, I32, I32, I32, I32, I32]),
         "plp_debug_sync_bound": (ctypes.c_int, [P, I32, I32]),
+        "plp_serve_counters": (ctypes.c_int, [P, P, P, P, P]),
         "plp_autotune": (ctypes.c_int, [P, P, I32, P, I32, I32, P]),
         "plp_batch_graph": (ctypes.c_int, [P]),
         "plp_solve": (ctypes.c_int, [P, P, I32, P, I32, P]),
@@ -339,6 +340,13 @@ class Handle:
 
     def set_tile(self, P: int = 0, C: int = 0, G: int = 0, D: int = 0, M: int = 0):
         _check(lib().plp_set_tile(self._p, P, C, G, D, M), self._p)
+
+    def serve_counters(self) -> dict:
+        """Serving launches, requests they served, re-runs on the wave path's
+        code, and eligible requests sent to the waves."""
+        v = [ctypes.c_int64() for _ in range(4)]
+        _check(lib().plp_serve_counters(self._p, *[ctypes.byref(x) for x in v]), self._p)
+        return dict(zip(("launches", "served", "fallbacks", "waved"), (x.value for x in v)))
 
     def debug_sync_bound(self, wait_limit: int = 0, skip_warp: int = -1):
         """Test hook of the multi-warp decoders' bounded barrier wait."""

@@ -107,3 +107,106 @@ def test_served_results_match_the_oracle_with_restart_budgets_64_256_1024():
         summ = res.summaries()
         key = lambda k: (not summ[k].fallback, summ[k].volume, summ[k].n_boxes, -k)
         assert res.best()[0] == max(range(R), key=key)
+
+
+def _thpack(L, W, H, types):
+    lines = ["1", "1 1", f"{L} {W} {H}", str(len(types))]
+    for i, (l, lf, w, wf, h, hf, q) in enumerate(types, 1):
+        lines.append(f"{i} {l} {lf} {w} {wf} {h} {hf} {q}")
+    return "\n".join(lines) + "\n"
+
+
+def _check_oracle(text, opts, res, stride=1):
+    oi = O.OInstance(text)
+    theta = None if opts.theta != opts.theta else opts.theta
+    for k in range(0, opts.restarts, stride):
+        js, _, _ = O.run(oi, seed=opts.seed + k, eps=opts.eps, theta=theta)
+        assert O.strip_time(res.json(k)) == O.strip_time(js), k
+
+
+def test_requests_join_one_persistent_launch():
+    """Staggered requests are served by the persistent serving launch (not
+    one launch each), and each result equals the synchronous solve's."""
+    reqs = _requests(32, seed=12)
+    insts = [P.Instance.parse(t) for t, _ in reqs]
+    with P.Handle() as h:
+        alone = [_jsons(h.solve([i], o)[0]) for i, (_, o) in zip(insts, reqs)]
+        ids = []
+        for i, (_, o) in zip(insts, reqs):
+            ids.append(h.submit(i, o))
+            time.sleep(0.0003)
+        for rid in ids:
+            assert h.wait(rid, 120000) == P.OK, P.last_error()
+        mixed = [_jsons(h.take(rid)) for rid in ids]
+        c = h.serve_counters()
+    assert mixed == alone
+    assert c["served"] == 32 and c["fallbacks"] == 0 and c["waved"] == 0
+    assert 1 <= c["launches"] <= 8
+
+
+def test_launch_configuration_changes_drain_and_relaunch():
+    """A container too tall for the running launch's top-z index, and
+    footprints too large for its 16-bit contact areas, wait for the launch to
+    drain and run in a relaunch with the merged configuration; every result
+    equals the oracle's."""
+    rng = random.Random(8)
+    tall = _thpack(50, 40, 5000, [(rng.randint(8, 25), 1, rng.randint(8, 20), 1, rng.randint(20, 90), 1,
+                                   rng.randint(20, 60)) for _ in range(4)])
+    wide = _thpack(1000, 1000, 100, [(300, 1, 300, 1, 40, 1, 9), (250, 1, 180, 1, 30, 1, 14),
+                                     (90, 1, 70, 1, 20, 1, 30)])
+    texts = [synth.batched(62000).to_thpack(), tall, synth.batched(62001).to_thpack(), wide,
+             synth.batched(62002).to_thpack()]
+    opts = [P.make_opts(seed=10 * i, restarts=6) for i in range(len(texts))]
+    with P.Handle() as h:
+        ids = [h.submit(P.Instance.parse(t), o) for t, o in zip(texts, opts)]
+        for rid in ids:
+            assert h.wait(rid, 120000) == P.OK, P.last_error()
+        res = [h.take(rid) for rid in ids]
+        c = h.serve_counters()
+    for t, o, r in zip(texts, opts, res):
+        _check_oracle(t, o, r)
+    assert c["served"] == 5 and c["launches"] >= 2
+
+
+def test_restarts_outgrowing_the_serving_tile_rerun_exactly():
+    """300 small boxes all fit, so a decode places more boxes than the serving
+    tile holds (256): the request runs again through the wave path's code,
+    with deeper tiles, and its results equal the oracle's."""
+    text = _thpack(587, 233, 220, [(20, 1, 20, 1, 20, 1, 300)])
+    o = P.make_opts(seed=3, restarts=3)
+    with P.Handle() as h:
+        rid = h.submit(P.Instance.parse(text), o)
+        assert h.wait(rid, 300000) == P.OK, P.last_error()
+        res = h.take(rid)
+        c = h.serve_counters()
+    assert c["fallbacks"] == 1
+    assert res.summary(0).n_boxes > 256
+    _check_oracle(text, o, res)
+
+
+def test_wave_path_when_serving_is_off(monkeypatch):
+    monkeypatch.setenv("PLP_SERVE", "0")
+    reqs = _requests(6, seed=14)
+    with P.Handle() as h:
+        ids = [h.submit(P.Instance.parse(t), o) for t, o in reqs]
+        for rid in ids:
+            assert h.wait(rid, 120000) == P.OK
+        res = [h.take(rid) for rid in ids]
+        assert h.serve_counters() == {"launches": 0, "served": 0, "fallbacks": 0, "waved": 0}
+    for (t, o), r in zip(reqs, res):
+        _check_oracle(t, o, r, stride=max(1, o.restarts // 4))
+
+
+def test_solve_after_serving_on_the_same_handle():
+    """The serving launch stops once idle, so a synchronous solve that
+    follows on the same handle runs and is exact."""
+    reqs = _requests(4, seed=15)
+    with P.Handle() as h:
+        ids = [h.submit(P.Instance.parse(t), o) for t, o in reqs]
+        for rid in ids:
+            assert h.wait(rid, 120000) == P.OK
+        t, o = reqs[0]
+        t0 = time.perf_counter()
+        r = h.solve([P.Instance.parse(t)], o)[0]
+        assert time.perf_counter() - t0 < 30
+        _check_oracle(t, o, r, stride=max(1, o.restarts // 4))
