@@ -119,6 +119,7 @@ void remember_tile(TileConfig& keep, const TileConfig& used) {
 
 
 constexpr int P_MAX = 2048;
+constexpr long long SEED_TABLE_MAX = 8192;   // seeded states kept per batch (2.5 KB each)
 constexpr int C_MAX = 8192;
 
 struct Batch;
@@ -335,12 +336,18 @@ struct Batch {
     // orientation's footprint area is below 65536, chosen (plan) when the
     // batch's restarts exceed one wave at 32-bit residency
     int sup16_ok = 1, sup16 = 0;
+    // seeded MT states computed once per distinct restart seed when the
+    // batch's restarts share seeds (every instance seeding 0 .. R - 1, say):
+    // seeds seed_lo .. seed_lo + seed_n - 1, or seed_n = 0 to seed in place
+    long long seed_lo = 0;
+    int seed_n = 0;
     std::vector<BlkShape> bcat;
     std::vector<int> btab;
     // device
     char* d_mem = nullptr;
     size_t bytes = 0;
-    size_t o_desc, o_steps, o_types, o_bcat, o_btab, o_work, o_next, o_heads, o_places, o_best, o_scratch, o_gather, o_redo;
+    size_t o_desc, o_steps, o_types, o_bcat, o_btab, o_work, o_next, o_heads, o_places, o_best, o_scratch, o_gather, o_redo,
+        o_seedtab;
     const uint32_t* mt_init = nullptr;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     char* h_flag = nullptr;                // pinned error-flag word
@@ -473,6 +480,21 @@ struct Batch {
         }
         // top-z index: one u16 per height level 0 .. H + 1 (binary search above 4094)
         Hz = maxH + 2 <= 4096 ? ((maxH + 2 + 7) & ~7) : 0;
+        // a table of seeded states pays when at least two restarts share each seed
+        seed_lo = 0;
+        seed_n = 0;
+        if (engine == 0 && !desc.empty()) {
+            long long lo = LLONG_MAX, hi = LLONG_MIN;
+            for (const auto& d : desc) {
+                lo = std::min(lo, d.seed);
+                hi = std::max(hi, d.seed + d.restarts - 1);
+            }
+            const long long span = hi - lo + 1;
+            if (span >= 1 && span <= SEED_TABLE_MAX && n_slots >= 2 * span) {
+                seed_lo = lo;
+                seed_n = (int)span;
+            }
+        }
         if (n_slots > INT_MAX / 2) return set_error(PLP_E_CAPACITY, "too many restarts in one batch");
         // longest instances first (dynamic scheduling then balances the tail)
         std::vector<int> order(in.size());
@@ -520,6 +542,7 @@ struct Batch {
         o_gather = o;  o = al(o + desc.size() * (size_t)max_stride * 8);
         o_scratch = o; o = al(o + std::max<size_t>(8, scratch_bytes));
         o_redo = o;    o = al(o + work.size() * sizeof(int2));
+        o_seedtab = o; o = al(o + (size_t)seed_n * 624 * sizeof(uint32_t));
         bytes = o;
     }
 
@@ -750,6 +773,8 @@ int batch_prepare(Batch& b, cudaStream_t st, Pinned& pin, int sms, const TileCon
     std::memcpy(pin.p + b.o_work, b.work.data(), b.work.size() * sizeof(int2));
     e = cudaMemcpyAsync(b.d_mem, pin.p, up, cudaMemcpyHostToDevice, st);
     if (e != cudaSuccess) return fail("batch upload", e);
+    e = launch_seed_table(b.seed_lo, b.seed_n, b.mt_init, reinterpret_cast<uint32_t*>(b.d_mem + b.o_seedtab), st);
+    if (e != cudaSuccess) return fail("seed table", e);
     // the staging buffer is reused by the next batch of this thread
     if (!one_shot) {
         e = cudaStreamSynchronize(st);
@@ -772,6 +797,9 @@ static DecodeLaunch make_launch(const Batch& b, const TileConfig& t, const int2*
     L.places = reinterpret_cast<unsigned long long*>(b.d_mem + b.o_places);
     L.scratch = reinterpret_cast<unsigned long long*>(b.d_mem + b.o_scratch);
     L.mt_init = b.mt_init;
+    L.seed_tab = b.seed_n ? reinterpret_cast<const uint32_t*>(b.d_mem + b.o_seedtab) : nullptr;
+    L.seed_lo = b.seed_lo;
+    L.seed_n = b.seed_n;
     L.P = t.P;
     L.C = t.C;
     L.Hz = b.Hz;

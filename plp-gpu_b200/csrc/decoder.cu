@@ -168,6 +168,9 @@ struct DecoderArgs {
     int P, C, Hz;
     int sync_limit;                // tries per barrier wait (0 = SYNC_WAIT_LIMIT)
     int sync_skip;                 // test hook: 1 + the warp that skips its first arrive
+    const uint32_t* seed_tab;      // seeded MT states of seeds seed_lo .. seed_lo + seed_n - 1 (or null)
+    long long seed_lo;
+    int seed_n;
 };
 
 
@@ -1353,7 +1356,15 @@ __device__ __forceinline__ void decoder1_body(const DecoderArgs& a, unsigned cha
         int mpos = 624;
         {
             const long long sd = I.seed + restart;
-            mt_seed_warp(mt, (unsigned long long)(sd < 0 ? -sd : sd), a.mt_init, lane);
+            if (!SERVE && a.seed_tab && sd >= a.seed_lo && sd - a.seed_lo < a.seed_n) {
+                // the seeded state, computed once for every restart of the batch with this seed
+                const uint4* src = reinterpret_cast<const uint4*>(a.seed_tab + (sd - a.seed_lo) * 624);
+                uint4* dst = reinterpret_cast<uint4*>(mt);
+                for (int i = lane; i < 156; i += 32) dst[i] = __ldg(src + i);
+                __syncwarp();
+            } else {
+                mt_seed_warp(mt, (unsigned long long)(sd < 0 ? -sd : sd), a.mt_init, lane);
+            }
         }
         const long long t0 = global_ns();   // the reference's run() clock starts after seeding
         int npass = 0;
@@ -1548,6 +1559,21 @@ __global__ void select_best_kernel(const InstDesc* __restrict__ inst, int n_inst
     const InstDesc I = inst[i];
     const int2 b = select_best_warp<false>(I, heads, lane);
     if (lane == 0) best[i] = b;
+}
+
+// ---------------------------------------------------------------------------
+// seeded MT19937 states of a range of seeds (one warp per seed), shared by
+// every restart of a batch that uses the same seed
+// ---------------------------------------------------------------------------
+__global__ void seed_table_kernel(long long lo, int n, const uint32_t* __restrict__ mt_init,
+                                  uint32_t* __restrict__ out) {
+    __shared__ uint32_t mts[4][624];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int i = blockIdx.x * 4 + w;
+    if (i >= n) return;
+    const long long sd = lo + i;
+    mt_seed_warp(mts[w], (unsigned long long)(sd < 0 ? -sd : sd), mt_init, lane);
+    for (int k = lane; k < 624; k += 32) out[(long long)i * 624 + k] = mts[w][k];
 }
 
 // ---------------------------------------------------------------------------
@@ -1775,6 +1801,9 @@ static DecoderArgs decoder_args(const DecodeLaunch& L) {
     a.Hz = L.Hz;
     a.sync_limit = L.sync_limit;
     a.sync_skip = L.sync_skip;
+    a.seed_tab = L.seed_tab;
+    a.seed_lo = L.seed_lo;
+    a.seed_n = L.seed_n;
     return a;
 }
 
@@ -1808,6 +1837,12 @@ cudaError_t launch_decoder(const DecodeLaunch& L, cudaStream_t st) {
     cudaError_t e = configure_decoder(L);
     if (e != cudaSuccess) return e;
     return enqueue_decoder(L, st);
+}
+
+cudaError_t launch_seed_table(long long lo, int n, const uint32_t* mt_init, uint32_t* out, cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    seed_table_kernel<<<(n + 3) / 4, 128, 0, st>>>(lo, n, mt_init, out);
+    return cudaGetLastError();
 }
 
 // ---- serving launches ------------------------------------------------------

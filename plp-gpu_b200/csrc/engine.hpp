@@ -34,7 +34,12 @@ struct DecodeLaunch {
     int ctas;
     int sync_limit;           // test hook: tries per barrier wait (0 = the kernel's bound)
     int sync_skip;            // test hook: 1 + the warp that skips its first arrive (0 = none)
+    const uint32_t* seed_tab; // seeded MT states of seeds seed_lo .. seed_lo + seed_n - 1 (null: seed in place)
+    long long seed_lo;
+    int seed_n;
 };
+// seeded MT states of seeds lo .. lo + n - 1, 624 words each
+cudaError_t launch_seed_table(long long lo, int n, const uint32_t* mt_init, uint32_t* out, cudaStream_t st);
 
 int decoder_smem_bytes(int P, int C, int Hz, int G, int sup16 = 0);   // sup16: 16-bit contact areas
 bool decoder_config_supported(int G, int D, int M);
