@@ -91,7 +91,7 @@ def test_every_reference_instance_eps0_matches_reference_host_and_is_valid():
         got = cli_rows(inst_path(r), GATE_FLAGS, [])[0]
         got.pop("time_s")
         assert got == r["expected"][0], r["name"]
-        L, W, H = map(int, open(inst_path(r)).read().split()[3:6])
+        (L, W, H), _, _ = P.Instance.load(inst_path(r)).info()
         check_valid(got["placements"], L, W, H)
 
 
