@@ -255,12 +255,15 @@ int plp_request_times(plp_handle* h, int64_t request_id, double* queued_s, doubl
  * and the decoder that finishes its last restart selects its best restart on
  * the device. Other requests run in waves on worker streams. PLP_SERVE=0 in
  * the environment when the first request arrives sends every request to the
- * waves. While the serving launch runs it holds the SMs: a synchronous solve
- * on the same GPU runs once the launch has stopped (about 5 ms after the last
+ * waves. A restart that outgrows the launch's tile is decoded again, inside
+ * the same launch, by one of its overflow decoders (a deeper tile in global
+ * memory). While the serving launch runs it holds the SMs: plp_solve,
+ * plp_batch_run and plp_autotune on this handle ask an idle launch to stop at
+ * once; other work on the GPU runs once it has stopped (50 ms after the last
  * request finished). This call reports the handle's serving launches,
  * requests served by them, requests re-run on the wave path's code after a
- * restart outgrew the serving tile, and eligible requests sent to the waves
- * (larger than the arena). */
+ * restart outgrew even the overflow tile, and eligible requests sent to the
+ * waves (larger than the arena or its staging). */
 int plp_serve_counters(plp_handle* h, int64_t* launches, int64_t* served, int64_t* fallbacks,
                        int64_t* waved);
 

@@ -13,6 +13,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <deque>
+#include <functional>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -1442,8 +1443,79 @@ void worker_main(plp_handle* h, int wi) {
 // run again on the wave path's code, which retries with deeper tiles.
 constexpr int SERVE_RING = 1 << 20;            // work items in flight at most
 constexpr int SERVE_RECORDS = 1 << 16;         // requests in flight at most
-constexpr double SERVE_IDLE_STOP_S = 0.005;
+constexpr double SERVE_IDLE_STOP_S = 0.05;
 constexpr int SERVE_IDLE_POLLS = 250000;       // about 1 s of empty polls per decoder
+constexpr int SERVE_DEEP_IDLE_POLLS = 8000000; // about a minute for an overflow decoder
+constexpr int SERVE_DEEP = 32;                 // overflow decoders per launch
+constexpr size_t SERVE_UP_STAGE = (size_t)32 << 20;     // pinned staging of uploads
+constexpr size_t SERVE_DOWN_STAGE = (size_t)256 << 20;  // pinned staging of results
+
+// Regions of one block freed in allocation order (the oldest first): a ring.
+// Free space is [newest end, cap) + [0, oldest start) until the newest region
+// lies before the oldest, then [newest end, oldest start).
+struct RegionRing {
+    struct R {
+        size_t off, end;
+        bool freed;
+    };
+    std::deque<R> live;
+    long long base = 0;                // id of live.front()
+    size_t cap = 0;
+    // first fit after the newest region (or from 0); -1 when it does not fit
+    long long place(size_t n, size_t* off, const std::function<bool(size_t, size_t)>& fits) {
+        if (live.empty()) {
+            if (!fits(0, cap)) return -1;
+            *off = 0;
+        } else {
+            const size_t oldest = live.front().off, newest_end = live.back().end;
+            const bool wrapped = live.back().off < oldest;
+            if (!wrapped && fits(newest_end, cap)) *off = newest_end;
+            else if (!wrapped && fits(0, oldest)) *off = 0;
+            else if (wrapped && fits(newest_end, oldest)) *off = newest_end;
+            else return -1;
+        }
+        (void)n;
+        return 0;
+    }
+    long long push(size_t off, size_t end) {
+        live.push_back({off, end, false});
+        return base + (long long)live.size() - 1;
+    }
+    void release(long long id) {
+        live[(size_t)(id - base)].freed = true;
+        while (!live.empty() && live.front().freed) {
+            live.pop_front();
+            base++;
+        }
+    }
+    void drop_newest() {
+        if (!live.empty()) live.pop_back();
+    }
+    void clear() {
+        base += (long long)live.size();
+        live.clear();
+    }
+};
+
+// A pinned block used as a RegionRing of 256-byte aligned chunks.
+struct PinnedRing {
+    char* p = nullptr;
+    RegionRing ring;
+    cudaError_t init(size_t cap) {
+        ring.cap = cap;
+        return cudaMallocHost(&p, cap);
+    }
+    ~PinnedRing() {
+        if (p) cudaFreeHost(p);
+    }
+    char* take(size_t n, long long* id) {
+        n = (n + 255) & ~(size_t)255;
+        size_t off = 0;
+        if (ring.place(n, &off, [&](size_t a, size_t b) { return a + n <= b; }) < 0) return nullptr;
+        *id = ring.push(off, off + n);
+        return p + off;
+    }
+};
 
 size_t serve_align(size_t x, size_t unit) {    // a multiple of unit and of 128 bytes
     size_t q = unit;
@@ -1452,7 +1524,8 @@ size_t serve_align(size_t x, size_t unit) {    // a multiple of unit and of 128 
 }
 
 struct ServeConfig {
-    int P = 256, C = 768, D = 1, M = 1, Hz = 0, sup16 = 0;
+    int P = 256, C = 512, D = 1, M = 12, Hz = 0, sup16 = 0;
+    int deep_P = 512, deep_C = 2048;   // the overflow decoders' tile (global memory)
     bool valid = false;
 };
 
@@ -1486,8 +1559,9 @@ struct ServeJob {
     long long region = -1;         // id of its arena region
     long long seq = 0;
     int slot = -1;
-    cudaEvent_t ev = nullptr;
-    std::shared_ptr<char> host;    // pinned: upload image, then [heads | places]
+    cudaEvent_t ev_up = nullptr, ev = nullptr;
+    long long up_id = -1, down_id = -1;   // staging regions
+    char* down = nullptr;                 // pinned staging of [heads | places]
     size_t up_bytes = 0, heads_bytes = 0, places_bytes = 0;
     double t0 = 0;
 };
@@ -1495,29 +1569,28 @@ struct ServeJob {
 struct ServeEngine {
     plp_handle* h;
     int device = 0, sms = 148;
-    std::shared_ptr<HostPool> pool;
     // device
     char* arena = nullptr;
     size_t cap = 0;
-    int* ctl = nullptr;            // [0] head, [1] tail, [2] stop, [3] error flag, [4] abort
+    // ctl: [0] head, [1] tail, [2] stop, [3] error flag, [4] abort, [5] overflow
+    // head, [6] overflow reservations, [7] main decoders alive
+    int* ctl = nullptr;
     int2* ring = nullptr;
+    int4* dring = nullptr;
+    unsigned char* deep_scratch = nullptr;
     // host
     long long* m_done_seq = nullptr;   // host-mapped completion records
     int2* m_done_best = nullptr;
-    int* h_word = nullptr;         // pinned: [0] head after a launch, [1 ..] tail values to copy
+    int* h_word = nullptr;         // pinned: [0..1] heads after a launch, [2] alive, [8 ..] tail values
+    PinnedRing up_stage, down_stage;
     ServeArgs args{};
     cudaStream_t up = nullptr, kern = nullptr, down = nullptr;
     cudaEvent_t ev_kern = nullptr, ev_go = nullptr;
     bool running = false, broken = false, stop_sent = false;
+    std::atomic<bool> yield_req{false};   // a synchronous call on the handle wants the SMs
     ServeConfig cfg;
     const uint32_t* mt_init = nullptr;
-    struct LiveRegion {
-        size_t off, end;
-        bool freed;
-    };
-    std::deque<LiveRegion> live;       // arena regions in allocation order
-    long long live_base = 0;           // region id of live.front()
-    size_t alloc_pos = 0;
+    RegionRing arena_ring;             // request regions of the arena
     std::deque<ServeJob*> pending;     // submitted, not yet taken by the engine (h->mu)
     std::deque<ServeJob*> fresh;       // taken, not yet admitted (engine thread)
     std::deque<ServeJob*> active;      // admitted (engine thread)
@@ -1537,24 +1610,31 @@ struct ServeEngine {
         return o.engine == 0 && o.passes == 1 && o.time_limit_s < 0 && !o.best_only;
     }
 
+    int deep_bytes() const { return decoder_smem_bytes(cfg.deep_P, cfg.deep_C, 4096, 1, 0); }
+
     int init(size_t arena_bytes) {
         device = h->device;
         sms = h->sms;
-        pool = h->pool;
         cudaError_t e = cudaSetDevice(device);
         if (e != cudaSuccess) return set_cuda_error("serving engine device", e);
         int status = PLP_OK;
         mt_init = device_mt_init(&status);
         if (!mt_init) return status;
         cap = arena_bytes;
+        arena_ring.cap = cap;
         e = cudaMalloc(&arena, cap);
         if (e == cudaSuccess) e = cudaMalloc(&ctl, 64);
         if (e == cudaSuccess) e = cudaMemset(ctl, 0, 64);
         if (e == cudaSuccess) e = cudaMalloc(&ring, sizeof(int2) * SERVE_RING);
+        if (e == cudaSuccess) e = cudaMalloc(&dring, sizeof(int4) * SERVE_RING);
+        if (e == cudaSuccess) e = cudaMemset(dring, 0, sizeof(int4) * SERVE_RING);
+        if (e == cudaSuccess) e = cudaMalloc(&deep_scratch, (size_t)SERVE_DEEP * deep_bytes());
         if (e == cudaSuccess)
             e = cudaHostAlloc(&m_done_seq, sizeof(long long) * SERVE_RECORDS, cudaHostAllocMapped);
         if (e == cudaSuccess) e = cudaHostAlloc(&m_done_best, sizeof(int2) * SERVE_RECORDS, cudaHostAllocMapped);
-        if (e == cudaSuccess) e = cudaMallocHost(&h_word, sizeof(int) * (1 + SERVE_RECORDS));
+        if (e == cudaSuccess) e = cudaMallocHost(&h_word, sizeof(int) * (8 + SERVE_RECORDS));
+        if (e == cudaSuccess) e = up_stage.init(SERVE_UP_STAGE);
+        if (e == cudaSuccess) e = down_stage.init(SERVE_DOWN_STAGE);
         for (cudaStream_t* s : {&up, &kern, &down})
             if (e == cudaSuccess) e = cudaStreamCreateWithFlags(s, cudaStreamNonBlocking);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev_kern, cudaEventDisableTiming);
@@ -1563,7 +1643,7 @@ struct ServeEngine {
         if (e == cudaSuccess) {
             for (int i = 0; i < SERVE_RECORDS; i++) m_done_seq[i] = -1;
             std::memset(m_done_best, 0, sizeof(int2) * SERVE_RECORDS);
-            h_word[0] = 0;
+            std::memset(h_word, 0, sizeof(int) * 8);
             e = cudaHostGetDevicePointer(&p, m_done_seq, 0);
         }
         args.done_seq = static_cast<volatile long long*>(p);
@@ -1576,8 +1656,16 @@ struct ServeEngine {
         args.ring = ring;
         args.ring_mask = SERVE_RING - 1;
         args.idle_polls = SERVE_IDLE_POLLS;
-        cfg.P = std::max(h->tile.P, 256);
-        cfg.C = std::max(h->tile.C, 768);
+        args.dring = dring;
+        args.dhead = ctl + 5;
+        args.dtail = ctl + 6;
+        args.alive = ctl + 7;
+        args.n_deep = SERVE_DEEP;
+        args.deep_P = cfg.deep_P;
+        args.deep_C = cfg.deep_C;
+        args.deep_bytes = deep_bytes();
+        args.deep_scratch = deep_scratch;
+        args.deep_idle_polls = SERVE_DEEP_IDLE_POLLS;
         th = std::thread([this] { loop(); });
         return PLP_OK;
     }
@@ -1596,10 +1684,7 @@ struct ServeEngine {
         }
         for (cudaStream_t s : {up, kern, down})
             if (s) cudaStreamSynchronize(s);
-        for (ServeJob* j : active) {
-            if (j->ev) cudaEventDestroy(j->ev);
-            delete j;
-        }
+        for (ServeJob* j : active) drop(j);
         for (ServeJob* j : fresh) delete j;
         for (ServeJob* j : pending) delete j;
         for (cudaStream_t s : {up, kern, down})
@@ -1608,8 +1693,14 @@ struct ServeEngine {
             if (v) cudaEventDestroy(v);
         for (void* q : {(void*)m_done_seq, (void*)m_done_best, (void*)h_word})
             if (q) cudaFreeHost(q);
-        for (void* q : {(void*)arena, (void*)ctl, (void*)ring})
+        for (void* q : {(void*)arena, (void*)ctl, (void*)ring, (void*)dring, (void*)deep_scratch})
             if (q) cudaFree(q);
+    }
+
+    void drop(ServeJob* j) {
+        for (cudaEvent_t v : {j->ev_up, j->ev})
+            if (v) cudaEventDestroy(v);
+        delete j;
     }
 
     // the stop word, in stream order on the upload stream
@@ -1619,36 +1710,12 @@ struct ServeEngine {
     }
 
     bool allocate(ServeJob& j) {
-        if (live.empty()) {
-            alloc_pos = 0;
-            if (!serve_layout(j.b, 0, cap, j.g)) return false;
-        } else {
-            const size_t oldest = live.front().off;
-            if (alloc_pos >= oldest) {         // free: [alloc_pos, cap) and [0, oldest)
-                if (!serve_layout(j.b, alloc_pos, cap, j.g) && !serve_layout(j.b, 0, oldest, j.g)) return false;
-            } else if (!serve_layout(j.b, alloc_pos, oldest, j.g)) {
-                return false;
-            }
-        }
-        alloc_pos = j.g.end;
-        live.push_back({j.g.off, j.g.end, false});
-        j.region = live_base + (long long)live.size() - 1;
+        size_t off = 0;
+        if (arena_ring.place(0, &off, [&](size_t a, size_t b) { return serve_layout(j.b, a, b, j.g); }) < 0)
+            return false;
+        serve_layout(j.b, off, cap, j.g);
+        j.region = arena_ring.push(j.g.off, j.g.end);
         return true;
-    }
-
-    void release(ServeJob& j) {
-        live[(size_t)(j.region - live_base)].freed = true;
-        while (!live.empty() && live.front().freed) {
-            live.pop_front();
-            live_base++;
-        }
-    }
-
-    void unallocate(ServeJob& j) {     // the newest region only
-        if (!live.empty() && j.region == live_base + (long long)live.size() - 1) {
-            live.pop_back();
-            alloc_pos = live.empty() ? 0 : live.back().end;
-        }
     }
 
     bool compatible(const Batch& b) const {
@@ -1709,12 +1776,18 @@ struct ServeEngine {
         cudaError_t e = serve_occupancy(cfg.P, cfg.C, cfg.Hz, cfg.D, cfg.M, cfg.sup16, &occ);
         if (e != cudaSuccess) return e;
         if (occ < 1) return cudaErrorInvalidConfiguration;
-        L.ctas = sms * occ;
+        L.ctas = std::max(sms * occ, SERVE_DEEP / cfg.D + 1);
+        // the overflow decoders' tile must hold this launch's top-z index
+        args.deep_bytes = decoder_smem_bytes(cfg.deep_P, cfg.deep_C, cfg.Hz, 1, cfg.sup16);
+        if (args.deep_bytes > deep_bytes()) return cudaErrorInvalidConfiguration;
+        h_word[2] = L.ctas * cfg.D - SERVE_DEEP;                  // main decoders
         send_stop(0);
-        e = cudaEventRecord(ev_go, up);                 // the launch follows every upload so far
+        e = cudaMemcpyAsync(ctl + 7, h_word + 2, sizeof(int), cudaMemcpyHostToDevice, up);
+        if (e == cudaSuccess) e = cudaEventRecord(ev_go, up);     // the launch follows every upload so far
         if (e == cudaSuccess) e = cudaStreamWaitEvent(kern, ev_go, 0);
         if (e == cudaSuccess) e = launch_serve(L, args, kern);
         if (e == cudaSuccess) e = cudaMemcpyAsync(h_word, ctl, sizeof(int), cudaMemcpyDeviceToHost, kern);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(h_word + 3, ctl + 5, 2 * sizeof(int), cudaMemcpyDeviceToHost, kern);
         if (e == cudaSuccess) e = cudaEventRecord(ev_kern, kern);
         if (e == cudaSuccess) {
             running = true;
@@ -1723,8 +1796,14 @@ struct ServeEngine {
         return e;
     }
 
+    // unclaimed work after the last launch ended: main items or overflow items
+    bool work_left() const {
+        const volatile int* w = h_word;
+        return w[0] < tail || w[3] < w[4];
+    }
+
     // tables, work items and the new tail of an admitted request, in one
-    // stream pass on the upload stream
+    // stream pass on the upload stream; false when the staging is full
     int publish(ServeJob& j) {
         const InstDesc& d0 = j.b.desc[0];
         const int R = d0.restarts;
@@ -1732,9 +1811,8 @@ struct ServeEngine {
         j.up_bytes = tab + (size_t)R * sizeof(int2);
         j.heads_bytes = (size_t)R * sizeof(SlotHead);
         j.places_bytes = (size_t)R * d0.place_stride * 8;
-        j.host = pool_take(pool, std::max(j.up_bytes, j.heads_bytes + j.places_bytes));
-        if (!j.host) return set_error(PLP_E_CAPACITY, "serving: no pinned host memory for a request");
-        char* img = j.host.get();
+        char* img = up_stage.take(j.up_bytes, &j.up_id);
+        if (!img) return PLP_E_PENDING;
         std::memset(img, 0, tab);
         InstDesc d = d0;
         d.step_off = (int)(j.g.steps / sizeof(int));
@@ -1759,16 +1837,19 @@ struct ServeEngine {
         if (e == cudaSuccess && first < R)
             e = cudaMemcpyAsync(ring, items + first, (R - first) * sizeof(int2), cudaMemcpyHostToDevice, up);
         tail += R;
-        int* src = h_word + 1 + (tail_copies++ % SERVE_RECORDS);
+        int* src = h_word + 8 + (tail_copies++ % SERVE_RECORDS);
         *src = tail;
         if (e == cudaSuccess) e = cudaMemcpyAsync(ctl + 1, src, sizeof(int), cudaMemcpyHostToDevice, up);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&j.ev_up, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventRecord(j.ev_up, up);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&j.ev, cudaEventDisableTiming);
         if (e != cudaSuccess) return set_cuda_error("serving upload", e);
         published += R;
         return PLP_OK;
     }
 
-    // the wave path's code, for a request whose restarts outgrew the serving tile
+    // the wave path's code, for a request whose restarts outgrew even the
+    // overflow decoders' tile
     void fallback(ServeJob& j) {
         if (running) {                 // the serving launch holds the SMs: let it finish its items
             send_stop(1);
@@ -1783,29 +1864,34 @@ struct ServeEngine {
         Batch b;
         const double t0 = now_seconds();
         int s = b.build({&j.inst}, {j.opts});
-        if (s == PLP_OK) s = run_batch(b, down, pin, sms, tile, &pool);
+        if (s == PLP_OK) s = run_batch(b, down, pin, sms, tile, &h->pool);
         std::vector<plp_result*> res;
         if (s == PLP_OK) res = collect(b, now_seconds() - t0);
         complete(j, s, s == PLP_OK ? res[0] : nullptr, s == PLP_OK ? "" : g_err);
     }
 
+    // the result, in ordinary host memory that it owns (the pinned staging is reused)
     plp_result* result_of(ServeJob& j) {
         const InstDesc& d = j.b.desc[0];
+        const size_t n = j.heads_bytes + j.places_bytes;
+        char* mem = static_cast<char*>(std::malloc(std::max<size_t>(n, 1)));
+        if (!mem) return nullptr;
+        std::memcpy(mem, j.down, n);
         auto* r = new plp_result;
         r->restarts = d.restarts;
         r->stride = d.place_stride;
         r->ors = j.b.inst_ors[0];
         r->L = d.L; r->W = d.W; r->H = d.H;
         r->steps = j.b.steps;
-        r->block = j.host;
-        r->heads = reinterpret_cast<const SlotHead*>(j.host.get());
+        r->block = std::shared_ptr<const char>(mem, [](const char* q) { std::free(const_cast<char*>(q)); });
+        r->heads = reinterpret_cast<const SlotHead*>(mem);
         r->seed0 = d.seed;
         r->time_s = now_seconds() - j.t0;
         const int2 best = m_done_best[j.slot];
         r->best = best.x;
         r->best_fallback = best.y;
         r->kept_all = true;
-        r->packed = reinterpret_cast<const unsigned long long*>(j.host.get() + j.heads_bytes);
+        r->packed = reinterpret_cast<const unsigned long long*>(mem + j.heads_bytes);
         return r;
     }
 
@@ -1816,20 +1902,17 @@ struct ServeEngine {
             h->queue.push_back(j->id);
         }
         h->cv_sched.notify_all();
-        delete j;
+        drop(j);
     }
 
     void fail_all(const std::string& why) {
         broken = true;
         for (ServeJob* j : active) {
             complete(*j, PLP_E_CUDA, nullptr, why);
-            if (j->ev) cudaEventDestroy(j->ev);
-            delete j;
+            drop(j);
         }
         active.clear();
-        live.clear();
-        live_base = 0;
-        alloc_pos = 0;
+        arena_ring.clear();
         for (ServeJob* j : fresh) route_to_waves(j);
         fresh.clear();
     }
@@ -1849,7 +1932,7 @@ struct ServeEngine {
             if (gone) {
                 fresh.pop_front();
                 h->cv.notify_all();
-                delete j;
+                drop(j);
                 progress = true;
                 continue;
             }
@@ -1863,7 +1946,10 @@ struct ServeEngine {
                 const int s = j->b.build({&j->inst}, {j->opts});
                 j->built = true;
                 ServeRegion whole;
-                if (s != PLP_OK || !serve_layout(j->b, 0, cap, whole) || j->b.desc[0].restarts > SERVE_RING / 4) {
+                if (s != PLP_OK || !serve_layout(j->b, 0, cap, whole) || j->b.desc[0].restarts > SERVE_RING / 4 ||
+                    (size_t)j->b.desc[0].restarts * (sizeof(SlotHead) + (size_t)j->b.desc[0].place_stride * 8) >
+                        SERVE_DOWN_STAGE / 2 ||
+                    whole.heads - whole.desc + (size_t)j->b.desc[0].restarts * sizeof(int2) > SERVE_UP_STAGE / 2) {
                     fresh.pop_front();               // errors and oversized requests: the wave path
                     route_to_waves(j);
                     progress = true;
@@ -1893,24 +1979,35 @@ struct ServeEngine {
                     j->r->t_start = j->t0;
                 }
             }
-            fresh.pop_front();
             if (gone) {                                // cancelled meanwhile: give the region back
-                unallocate(*j);
-                delete j;
+                fresh.pop_front();
+                arena_ring.drop_newest();
+                drop(j);
+                progress = true;
+                continue;
+            }
+            const int save_tail = tail;
+            const long long save_seq = next_seq;
+            j->seq = next_seq++;
+            j->slot = (int)(j->seq % SERVE_RECORDS);
+            const int s = publish(*j);
+            if (s == PLP_E_PENDING) {                  // upload staging full: try again later
+                next_seq = save_seq;
+                tail = save_tail;
+                arena_ring.drop_newest();
+                std::lock_guard<std::mutex> lk(h->mu);
+                j->r->running = false;
+                break;
+            }
+            fresh.pop_front();
+            if (s != PLP_OK) {
+                arena_ring.drop_newest();
+                complete(*j, s, nullptr, g_err);
+                drop(j);
                 progress = true;
                 continue;
             }
             merge_config(j->b);
-            j->seq = next_seq++;
-            j->slot = (int)(j->seq % SERVE_RECORDS);
-            const int s = publish(*j);
-            if (s != PLP_OK) {
-                unallocate(*j);
-                complete(*j, s, nullptr, g_err);
-                delete j;
-                progress = true;
-                continue;
-            }
             j->state = 1;
             active.push_back(j);
             progress = true;
@@ -1921,12 +2018,18 @@ struct ServeEngine {
     // one pass of the scheduler; true when something changed
     bool step() {
         bool progress = admit();
+        // upload staging comes back once its copies have run
+        for (ServeJob* j : active)
+            if (j->up_id >= 0 && cudaEventQuery(j->ev_up) == cudaSuccess) {
+                up_stage.ring.release(j->up_id);
+                j->up_id = -1;
+            }
         // the launch: started again whenever published work is unclaimed
         if (running && cudaEventQuery(ev_kern) == cudaSuccess) {
             running = false;
             progress = true;
         }
-        if (!running && !broken && *reinterpret_cast<volatile int*>(h_word) < tail) {
+        if (!running && !broken && work_left()) {
             const cudaError_t e = launch();
             if (e != cudaSuccess) {
                 cudaGetLastError();
@@ -1939,10 +2042,12 @@ struct ServeEngine {
         for (ServeJob* j : active) {
             if (j->state != 1) continue;
             if (__atomic_load_n(&m_done_seq[j->slot], __ATOMIC_ACQUIRE) != j->seq) continue;
-            cudaError_t e = cudaMemcpyAsync(j->host.get(), arena + j->g.heads, j->heads_bytes,
+            j->down = down_stage.take(j->heads_bytes + j->places_bytes, &j->down_id);
+            if (!j->down) break;                       // staging full: later
+            cudaError_t e = cudaMemcpyAsync(j->down, arena + j->g.heads, j->heads_bytes,
                                             cudaMemcpyDeviceToHost, down);
             if (e == cudaSuccess)
-                e = cudaMemcpyAsync(j->host.get() + j->heads_bytes, arena + j->g.places, j->places_bytes,
+                e = cudaMemcpyAsync(j->down + j->heads_bytes, arena + j->g.places, j->places_bytes,
                                     cudaMemcpyDeviceToHost, down);
             if (e == cudaSuccess) e = cudaEventRecord(j->ev, down);
             if (e != cudaSuccess) {
@@ -1956,37 +2061,42 @@ struct ServeEngine {
         }
         for (auto it = active.begin(); it != active.end();) {
             ServeJob* j = *it;
-            if (j->state != 2 || cudaEventQuery(j->ev) != cudaSuccess) {
+            if (j->state != 2 || j->up_id >= 0 || cudaEventQuery(j->ev) != cudaSuccess) {
                 ++it;
                 continue;
             }
-            const SlotHead* hd = reinterpret_cast<const SlotHead*>(j->host.get());
+            const SlotHead* hd = reinterpret_cast<const SlotHead*>(j->down);
             bool overflow = false;
             for (int k = 0; k < j->b.desc[0].restarts; k++) overflow = overflow || hd[k].err != ERR_NONE;
-            release(*j);
-            cudaEventDestroy(j->ev);
-            j->ev = nullptr;
+            arena_ring.release(j->region);
             if (overflow) {
+                down_stage.ring.release(j->down_id);
                 n_fallbacks++;
                 fallback(*j);
             } else {
+                plp_result* res = result_of(*j);
+                down_stage.ring.release(j->down_id);
                 n_served++;
-                complete(*j, PLP_OK, result_of(*j), "");
+                if (res) complete(*j, PLP_OK, res, "");
+                else complete(*j, PLP_E_CAPACITY, nullptr, "serving: no host memory for a result");
             }
-            delete j;
+            drop(j);
             it = active.erase(it);
             progress = true;
         }
         // idle: stop the launch; with nothing in flight the counters restart at 0
         const double now = now_seconds();
         if (progress || !active.empty() || !fresh.empty()) last_busy = now;
-        if (running && !stop_sent && active.empty() && fresh.empty() && now - last_busy > SERVE_IDLE_STOP_S)
+        const bool idle = active.empty() && fresh.empty();
+        if (running && !stop_sent && idle && (now - last_busy > SERVE_IDLE_STOP_S || yield_req.load()))
             send_stop(1);
-        if (!running && active.empty() && fresh.empty() && tail > (1 << 30)) {
-            cudaMemsetAsync(ctl, 0, 2 * sizeof(int), up);
+        if (!running) yield_req = false;
+        if (!running && idle && (tail > (1 << 30) || h_word[4] > (1 << 30)) && !work_left()) {
+            cudaMemsetAsync(ctl, 0, 2 * sizeof(int), up);        // head, tail
+            cudaMemsetAsync(ctl + 5, 0, 2 * sizeof(int), up);    // overflow head, reservations
             cudaStreamSynchronize(up);
             tail = 0;
-            h_word[0] = 0;
+            h_word[0] = h_word[3] = h_word[4] = 0;
         }
         return progress;
     }
@@ -2012,6 +2122,13 @@ struct ServeEngine {
         }
     }
 };
+
+// A synchronous call on the handle is about to launch: an idle serving
+// launch stops now instead of after SERVE_IDLE_STOP_S, so the SMs free up.
+void serve_yield(plp_handle* h) {
+    std::lock_guard<std::mutex> g(h->serve_mu);
+    if (h->serve) h->serve->yield_req = true;
+}
 
 // The handle's serving engine, made on first use. Its arena is half the
 // budget, at most PLP_SERVE_ARENA_MB (default 4096 MiB), reserved from the
@@ -2424,6 +2541,7 @@ int plp_autotune(plp_handle* h, const plp_instance* const* insts, int32_t n_inst
         record(h, s);
         return s;
     }
+    serve_yield(h);
     std::vector<const Instance*> in;
     std::vector<plp_run_opts> op;
     for (int i = 0; i < n_inst; i++) {
@@ -2527,6 +2645,7 @@ int plp_solve(plp_handle* h, const plp_instance* const* insts, int32_t n_inst,
         record(h, s);
         return s;
     }
+    serve_yield(h);
     std::lock_guard<std::mutex> g(h->sync_mu);
     cudaSetDevice(h->device);
     std::vector<const Instance*> in;
@@ -2750,6 +2869,7 @@ int plp_batch_prepare(plp_handle* h, const plp_instance* const* insts, int32_t n
 int plp_batch_run(plp_batch* pb, double* device_ms, double* decoder_ms, int32_t* launches) {
     if (!pb) return set_error(PLP_E_INVALID, "plp_batch_run: null batch");
     plp_handle* h = pb->h;
+    serve_yield(h);
     std::lock_guard<std::mutex> g(h->sync_mu);
     cudaSetDevice(h->device);
     TileConfig tile;

@@ -1205,6 +1205,57 @@ __device__ __forceinline__ void st_release_sys(volatile long long* p, long long 
     asm volatile("st.release.sys.b64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
+__device__ __forceinline__ void st_release_gpu(int* p, int v) {
+    asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Lane 0 of an overflow decoder: the next overflow item (ticket), or -1 once
+// the host asked the launch to stop and every main decoder has exited with
+// nothing left, or after deep_idle_polls empty polls.
+__device__ __forceinline__ int serve_claim_deep(const ServeArgs& s) {
+    unsigned ns = 64;
+    for (int k = 0; k < s.deep_idle_polls; k++) {
+        const int t = ld_acquire_gpu(s.dtail);
+        int h = *reinterpret_cast<volatile int*>(s.dhead);
+        while (h < t) {
+            const int prev = atomicCAS(s.dhead, h, h + 1);
+            if (prev == h) return h;
+            h = prev;
+        }
+        // main decoders push before they leave, so once none is left the
+        // reservation count seen after that is final
+        if (ld_acquire_gpu(s.stop) && ld_acquire_gpu(s.alive) == 0 && ld_acquire_gpu(s.dtail) <= h) return -1;
+        __nanosleep(ns);
+        if (ns < 8192) ns <<= 1;
+    }
+    return -1;
+}
+
+// Lane 0: waits (bounded) until the producer of ticket t has written it.
+__device__ __forceinline__ bool serve_deep_item(const ServeArgs& s, int t, int2* w) {
+    int4* e = s.dring + (t & s.ring_mask);
+    for (int k = 0; k < (1 << 22); k++) {
+        if (ld_acquire_gpu(&e->z) == t + 1) {
+            *w = make_int2(*reinterpret_cast<volatile int*>(&e->x), *reinterpret_cast<volatile int*>(&e->y));
+            return true;
+        }
+        __nanosleep(32);
+    }
+    return false;
+}
+
+// A main decoder hands a restart that outgrew its tile to the overflow ring.
+__device__ __forceinline__ void serve_push_deep(const ServeArgs& s, int2 wk, int lane) {
+    if (lane == 0) {
+        const int t = atomicAdd(s.dtail, 1);
+        int4* e = s.dring + (t & s.ring_mask);
+        *reinterpret_cast<volatile int*>(&e->x) = wk.x;
+        *reinterpret_cast<volatile int*>(&e->y) = wk.y;
+        st_release_gpu(&e->z, t + 1);
+    }
+    __syncwarp();
+}
+
 // Lane 0: claims the next published work item, or returns -1 once the host
 // has asked the launch to stop (and nothing is left) or after idle_polls
 // empty polls. The host publishes by stream-ordered copies into device
@@ -1302,7 +1353,10 @@ __device__ __forceinline__ void serve_finish(const DecoderArgs& a, const ServeAr
     __syncwarp();
 }
 
-template <typename SupT, bool SERVE>
+// MODE 0: batch launch; 1: serving launch, main decoder (pushes restarts
+// that outgrow its tile to the overflow ring); 2: serving launch, overflow
+// decoder (deeper tile in global memory, takes the overflow ring).
+template <typename SupT, int MODE>
 __device__ __forceinline__ void decoder1_body(const DecoderArgs& a, unsigned char* base, int gdec,
                                               const ServeArgs& sv) {
     const int lane = threadIdx.x & 31;
@@ -1320,16 +1374,28 @@ __device__ __forceinline__ void decoder1_body(const DecoderArgs& a, unsigned cha
     unsigned short* wi = reinterpret_cast<unsigned short*>(base + lay.off_wi);
     unsigned short* zt = a.Hz ? reinterpret_cast<unsigned short*>(base + lay.off_zt) : nullptr;
 
+    constexpr bool SERVE = MODE != 0;
     const int n_work = SERVE ? 0 : (a.n_work_dev ? *a.n_work_dev : a.n_work);
     for (;;) {
-        if (*reinterpret_cast<volatile int*>(a.abort)) return;
+        if (*reinterpret_cast<volatile int*>(a.abort)) break;
         int2 wk;
         if (SERVE) {
             int item = -1, wx = 0, wy = 0;
             if (lane == 0) {
-                item = serve_claim(sv);
-                if (item >= 0) {
-                    const int2 w = ld_relaxed_gpu_int2(sv.ring + (item & sv.ring_mask));
+                if (MODE == 1) {
+                    item = serve_claim(sv);
+                    if (item >= 0) {
+                        const int2 w = ld_relaxed_gpu_int2(sv.ring + (item & sv.ring_mask));
+                        wx = w.x;
+                        wy = w.y;
+                    }
+                } else {
+                    item = serve_claim_deep(sv);
+                    int2 w = make_int2(0, 0);
+                    if (item >= 0 && !serve_deep_item(sv, item, &w)) {
+                        atomicOr(a.err_flag, 1 << ERR_SYNC);   // a producer never finished its item
+                        item = -1;
+                    }
                     wx = w.x;
                     wy = w.y;
                 }
@@ -1511,7 +1577,10 @@ __device__ __forceinline__ void decoder1_body(const DecoderArgs& a, unsigned cha
             // wall-clock budget (gpu/plp_common.hpp:484-492): stop once it is spent
             if (I.budget_ns >= 0 && __shfl_sync(FULL, global_ns() - t0, 0) >= I.budget_ns) break;
         }
-        if (lane == 0) {
+        // a serving main decoder hands a restart that outgrew its tile to the
+        // launch's overflow decoders instead of reporting it
+        const bool to_deep = MODE == 1 && (err == ERR_BOX_CAP || err == ERR_CAND_CAP);
+        if (lane == 0 && !to_deep) {
             if (err) atomicOr(a.err_flag, 1 << err);
             SlotHead h;
             h.n_boxes = err ? 0 : best_n;
@@ -1523,7 +1592,12 @@ __device__ __forceinline__ void decoder1_body(const DecoderArgs& a, unsigned cha
             a.heads[slot] = h;
         }
         __syncwarp();
-        if (SERVE) serve_finish(a, sv, wk.x, I, lane);
+        if (to_deep) serve_push_deep(sv, wk, lane);
+        else if (SERVE) serve_finish(a, sv, wk.x, I, lane);
+    }
+    if (MODE == 1 && lane == 0) {   // pushes above are visible before the count drops
+        __threadfence();
+        atomicSub(sv.alive, 1);
     }
 }
 
@@ -1534,7 +1608,7 @@ __global__ void __launch_bounds__(32 * D, M) decoder1_kernel(DecoderArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int dec = threadIdx.x >> 5;
     const Dec1Layout lay = dec1_layout(a.P, a.C, a.Hz, (int)sizeof(SupT));
-    decoder1_body<SupT, false>(a, smem_raw + (size_t)dec * lay.bytes, blockIdx.x * D + dec, ServeArgs{});
+    decoder1_body<SupT, 0>(a, smem_raw + (size_t)dec * lay.bytes, blockIdx.x * D + dec, ServeArgs{});
 }
 
 // The serving launch: the single-warp decoder over the host-published ring.
@@ -1543,8 +1617,16 @@ __global__ void __launch_bounds__(32 * D, M) serve_kernel(DecoderArgs a, ServeAr
     using SupT = typename std::conditional<S16 != 0, unsigned short, int>::type;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int dec = threadIdx.x >> 5;
-    const Dec1Layout lay = dec1_layout(a.P, a.C, a.Hz, (int)sizeof(SupT));
-    decoder1_body<SupT, true>(a, smem_raw + (size_t)dec * lay.bytes, blockIdx.x * D + dec, s);
+    const int gdec = blockIdx.x * D + dec;
+    if (gdec < s.n_deep) {
+        DecoderArgs ad = a;
+        ad.P = s.deep_P;
+        ad.C = s.deep_C;
+        decoder1_body<SupT, 2>(ad, s.deep_scratch + (size_t)gdec * s.deep_bytes, gdec, s);
+    } else {
+        const Dec1Layout lay = dec1_layout(a.P, a.C, a.Hz, (int)sizeof(SupT));
+        decoder1_body<SupT, 1>(a, smem_raw + (size_t)dec * lay.bytes, gdec, s);
+    }
 }
 
 // ---------------------------------------------------------------------------

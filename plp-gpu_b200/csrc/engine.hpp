@@ -85,6 +85,16 @@ struct ServeArgs {
     volatile long long* done_seq;   // host-mapped: per completion record, the finished request's seq
     int2* done_best;                // host-mapped: per completion record, (best restart, fallback)
     int idle_polls;                 // empty polls before a decoder exits (about 4 us each)
+    // Restarts that outgrow the launch's tile are pushed by their decoder onto
+    // the overflow ring and decoded again by the launch's first n_deep
+    // decoders, whose deeper tile (deep_P, deep_C) lives in global memory.
+    int4* dring;                    // device: {descriptor, restart, ticket + 1, 0}, ring_mask + 1 entries
+    int* dhead;                     // device: overflow items claimed
+    int* dtail;                     // device: overflow items reserved
+    int* alive;                     // device: main decoders of the launch not yet exited
+    int n_deep, deep_P, deep_C, deep_bytes;
+    unsigned char* deep_scratch;    // device: n_deep x deep_bytes
+    int deep_idle_polls;            // empty polls before an overflow decoder exits
 };
 bool serve_config_supported(int D, int M);
 cudaError_t serve_occupancy(int P, int C, int Hz, int D, int M, int sup16, int* ctas_per_sm);

@@ -168,19 +168,40 @@ def test_launch_configuration_changes_drain_and_relaunch():
     assert c["served"] == 5 and c["launches"] >= 2
 
 
-def test_restarts_outgrowing_the_serving_tile_rerun_exactly():
+def test_restarts_outgrowing_the_serving_tile_go_to_the_overflow_decoders():
     """300 small boxes all fit, so a decode places more boxes than the serving
-    tile holds (256): the request runs again through the wave path's code,
-    with deeper tiles, and its results equal the oracle's."""
+    tile holds (256): its decoder hands the restart to the launch's overflow
+    decoders (a 512-box tile in global memory) inside the same launch. The
+    results equal the oracle's, and a normal request served beside it too."""
     text = _thpack(587, 233, 220, [(20, 1, 20, 1, 20, 1, 300)])
-    o = P.make_opts(seed=3, restarts=3)
+    normal = synth.batched(62010).to_thpack()
+    o, on = P.make_opts(seed=3, restarts=3), P.make_opts(seed=9, restarts=16)
+    with P.Handle() as h:
+        rid = h.submit(P.Instance.parse(text), o)
+        rn = h.submit(P.Instance.parse(normal), on)
+        assert h.wait(rid, 300000) == P.OK, P.last_error()
+        assert h.wait(rn, 300000) == P.OK, P.last_error()
+        res, resn = h.take(rid), h.take(rn)
+        c = h.serve_counters()
+    assert c["fallbacks"] == 0 and c["served"] == 2
+    assert res.summary(0).n_boxes > 256
+    _check_oracle(text, o, res)
+    _check_oracle(normal, on, resn, stride=3)
+
+
+def test_restarts_outgrowing_the_overflow_tile_rerun_on_the_wave_path():
+    """600 boxes outgrow the overflow decoders' 512-box tile as well: the
+    request runs again through the wave path's code, with deeper tiles, and
+    its results equal the oracle's."""
+    text = _thpack(587, 233, 220, [(10, 1, 10, 1, 10, 1, 600)])
+    o = P.make_opts(seed=5, restarts=2)
     with P.Handle() as h:
         rid = h.submit(P.Instance.parse(text), o)
         assert h.wait(rid, 300000) == P.OK, P.last_error()
         res = h.take(rid)
         c = h.serve_counters()
     assert c["fallbacks"] == 1
-    assert res.summary(0).n_boxes > 256
+    assert res.summary(0).n_boxes > 512
     _check_oracle(text, o, res)
 
 
