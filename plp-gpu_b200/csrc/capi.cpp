@@ -361,6 +361,7 @@ struct Batch {
     // one-graph replay of a clean execution (flag reset, decoder, flag copy,
     // select, gather), kept for later executions with the same tile
     cudaGraphExec_t gexec = nullptr;
+    cudaGraphExec_t gexec2 = nullptr;      // the part after the first decoder (retry stage, flags, select)
     TileConfig gtile;
     int glaunches = 0;
     bool gstaged = false;                  // the graph holds the device retry stage
@@ -714,6 +715,10 @@ int batch_release(Batch& b, cudaStream_t st) {
         cudaGraphExecDestroy(b.gexec);
         b.gexec = nullptr;
     }
+    if (b.gexec2) {
+        cudaGraphExecDestroy(b.gexec2);
+        b.gexec2 = nullptr;
+    }
     cudaError_t e = cudaSuccess;
     if (b.d_mem) e = cudaFreeAsync(b.d_mem, st);
     b.d_mem = nullptr;
@@ -921,13 +926,18 @@ int pending_bits(const Batch& b, bool staged) {
 
 // Records a clean execution of the batch with tile t as one CUDA graph:
 // error-flag reset, the persistent decoder, the retry stage where it applies,
-// the flag copy to the pinned words, selection and gather, with events ev[3]
-// and ev[1] around the first decoder (the decoder's own time under replay). A capture that fails leaves the batch on direct
+// the flag copy to the pinned words, selection and gather, as two graphs
+// (the first ends after the first decoder, so an event between their
+// launches gives the decoder's own time under replay). A capture that fails leaves the batch on direct
 // launches.
 void batch_capture(Batch& b, cudaStream_t st, int sms, const TileConfig& t) {
     if (b.gexec) {
         cudaGraphExecDestroy(b.gexec);
         b.gexec = nullptr;
+    }
+    if (b.gexec2) {
+        cudaGraphExecDestroy(b.gexec2);
+        b.gexec2 = nullptr;
     }
     // launch shapes and function attributes: before capture
     const DecodeLaunch L = make_launch(b, t, reinterpret_cast<const int2*>(b.d_mem + b.o_work),
@@ -947,30 +957,42 @@ void batch_capture(Batch& b, cudaStream_t st, int sms, const TileConfig& t) {
         }
     }
     char* d_flag = b.d_mem + b.o_next + 8;
-    if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+    // two graphs, so that events recorded between their launches time the
+    // decoder alone: [flag reset, decoder] and [retry stage, flag copy, select]
+    cudaGraph_t g = nullptr, g2 = nullptr;
+    int n = 0;
+    cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) {
         cudaGetLastError();
         return;
     }
-    int n = 0;
-    cudaError_t e = cudaMemsetAsync(d_flag, 0, 16, st);
-    if (e == cudaSuccess) e = cudaEventRecord(b.ev[3], st);
+    e = cudaMemsetAsync(d_flag, 0, 16, st);
     if (e == cudaSuccess) e = enqueue_decoder(L, st);
     if (e == cudaSuccess) n++;
-    if (e == cudaSuccess) e = cudaEventRecord(b.ev[1], st);
-    if (e == cudaSuccess && staged) e = enqueue_redo(b, L2, sms, st, &n);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(b.h_flag, d_flag, 16, cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess) e = enqueue_select(b, st, &n);
-    cudaGraph_t g = nullptr;
-    const cudaError_t e2 = cudaStreamEndCapture(st, &g);
-    if (e == cudaSuccess && e2 == cudaSuccess && g) {
-        cudaGraphExec_t x = nullptr;
-        if (cudaGraphInstantiate(&x, g, 0) == cudaSuccess) {
+    cudaError_t e2 = cudaStreamEndCapture(st, &g);
+    if (e == cudaSuccess && e2 == cudaSuccess) {
+        e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            if (staged) e = enqueue_redo(b, L2, sms, st, &n);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(b.h_flag, d_flag, 16, cudaMemcpyDeviceToHost, st);
+            if (e == cudaSuccess) e = enqueue_select(b, st, &n);
+            e2 = cudaStreamEndCapture(st, &g2);
+        }
+    }
+    if (e == cudaSuccess && e2 == cudaSuccess && g && g2) {
+        cudaGraphExec_t x = nullptr, x2 = nullptr;
+        if (cudaGraphInstantiate(&x, g, 0) == cudaSuccess && cudaGraphInstantiate(&x2, g2, 0) == cudaSuccess) {
             b.gexec = x;
+            b.gexec2 = x2;
             b.gtile = t;
             b.glaunches = n;
             b.gstaged = staged;
+        } else {
+            if (x) cudaGraphExecDestroy(x);
+            if (x2) cudaGraphExecDestroy(x2);
         }
     }
+    if (g2) cudaGraphDestroy(g2);
     if (g) cudaGraphDestroy(g);
     cudaGetLastError();
 }
@@ -1043,6 +1065,8 @@ int batch_execute(Batch& b, cudaStream_t st, int sms, TileConfig& tile, ExecStat
         // replay: one graph launch, one synchronisation
         cudaError_t e = cudaEventRecord(b.ev[0], st);
         if (e == cudaSuccess) e = cudaGraphLaunch(b.gexec, st);
+        if (e == cudaSuccess) e = cudaEventRecord(b.ev[1], st);
+        if (e == cudaSuccess) e = cudaGraphLaunch(b.gexec2, st);
         if (e == cudaSuccess) e = cudaEventRecord(b.ev[2], st);
         if (e == cudaSuccess && rc) e = result_enqueue(b, *rc, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
@@ -1050,7 +1074,7 @@ int batch_execute(Batch& b, cudaStream_t st, int sms, TileConfig& tile, ExecStat
         if (pending_bits(b, b.gstaged) == 0) {
             float ms = 0, dms = 0;
             cudaEventElapsedTime(&ms, b.ev[0], b.ev[2]);
-            if (cudaEventElapsedTime(&dms, b.ev[3], b.ev[1]) != cudaSuccess) {
+            if (cudaEventElapsedTime(&dms, b.ev[0], b.ev[1]) != cudaSuccess) {
                 cudaGetLastError();
                 dms = ms;
             }
