@@ -1605,7 +1605,8 @@ struct ServeEngine {
     // host
     long long* m_done_seq = nullptr;   // host-mapped completion records
     int2* m_done_best = nullptr;
-    int* h_word = nullptr;         // pinned: [0..1] heads after a launch, [2] alive, [8 ..] tail values
+    int* h_word = nullptr;         // pinned: [0] head and [3..4] overflow head and reservations after a
+                                   // launch, [2] main decoders, [5] 1 and [6] 0 (stop), [8 ..] tail values
     PinnedRing up_stage, down_stage;
     ServeArgs args{};
     cudaStream_t up = nullptr, kern = nullptr, down = nullptr;
@@ -1668,6 +1669,8 @@ struct ServeEngine {
             for (int i = 0; i < SERVE_RECORDS; i++) m_done_seq[i] = -1;
             std::memset(m_done_best, 0, sizeof(int2) * SERVE_RECORDS);
             std::memset(h_word, 0, sizeof(int) * 8);
+            h_word[5] = 1;                 // stop word sources (never written again)
+            h_word[6] = 0;
             e = cudaHostGetDevicePointer(&p, m_done_seq, 0);
         }
         args.done_seq = static_cast<volatile long long*>(p);
@@ -1727,9 +1730,12 @@ struct ServeEngine {
         delete j;
     }
 
-    // the stop word, in stream order on the upload stream
+    // The stop word, in stream order on the upload stream, as a copy from a
+    // pinned constant: a copy runs on a copy engine while the serving launch
+    // holds every SM, where a memset (which may run as a kernel) would wait
+    // for the launch to end.
     void send_stop(int v) {
-        cudaMemsetAsync(ctl + 2, v ? 1 : 0, sizeof(int), up);
+        cudaMemcpyAsync(ctl + 2, h_word + (v ? 5 : 6), sizeof(int), cudaMemcpyHostToDevice, up);
         stop_sent = v != 0;
     }
 
