@@ -1470,7 +1470,7 @@ constexpr int SERVE_RECORDS = 1 << 16;         // requests in flight at most
 constexpr double SERVE_IDLE_STOP_S = 0.05;
 constexpr int SERVE_IDLE_POLLS = 250000;       // about 1 s of empty polls per decoder
 constexpr int SERVE_DEEP_IDLE_POLLS = 8000000; // about a minute for an overflow decoder
-constexpr int SERVE_DEEP = 32;                 // overflow decoders per launch
+constexpr int SERVE_DEEP = 32;                 // overflow decoders per launch (PLP_SERVE_DEEP overrides)
 constexpr size_t SERVE_UP_STAGE = (size_t)32 << 20;     // pinned staging of uploads
 constexpr size_t SERVE_DOWN_STAGE = (size_t)256 << 20;  // pinned staging of results
 
@@ -1612,6 +1612,7 @@ struct ServeEngine {
     cudaStream_t up = nullptr, kern = nullptr, down = nullptr;
     cudaEvent_t ev_kern = nullptr, ev_go = nullptr;
     bool running = false, broken = false, stop_sent = false;
+    int n_deep = 0;                       // overflow decoders per launch
     std::atomic<bool> yield_req{false};   // a synchronous call on the handle wants the SMs
     ServeConfig cfg;
     const uint32_t* mt_init = nullptr;
@@ -1653,7 +1654,13 @@ struct ServeEngine {
         if (e == cudaSuccess) e = cudaMalloc(&ring, sizeof(int2) * SERVE_RING);
         if (e == cudaSuccess) e = cudaMalloc(&dring, sizeof(int4) * SERVE_RING);
         if (e == cudaSuccess) e = cudaMemset(dring, 0, sizeof(int4) * SERVE_RING);
-        if (e == cudaSuccess) e = cudaMalloc(&deep_scratch, (size_t)SERVE_DEEP * deep_bytes());
+        n_deep = SERVE_DEEP;
+        if (const char* v = std::getenv("PLP_SERVE_DEEP")) {
+            char* end = nullptr;
+            const long x = std::strtol(v, &end, 10);
+            if (end != v && x >= 0 && x <= 1024) n_deep = (int)x;
+        }
+        if (e == cudaSuccess) e = cudaMalloc(&deep_scratch, (size_t)std::max(1, n_deep) * deep_bytes());
         if (e == cudaSuccess)
             e = cudaHostAlloc(&m_done_seq, sizeof(long long) * SERVE_RECORDS, cudaHostAllocMapped);
         if (e == cudaSuccess) e = cudaHostAlloc(&m_done_best, sizeof(int2) * SERVE_RECORDS, cudaHostAllocMapped);
@@ -1687,7 +1694,7 @@ struct ServeEngine {
         args.dhead = ctl + 5;
         args.dtail = ctl + 6;
         args.alive = ctl + 7;
-        args.n_deep = SERVE_DEEP;
+        args.n_deep = n_deep;
         args.deep_P = cfg.deep_P;
         args.deep_C = cfg.deep_C;
         args.deep_bytes = deep_bytes();
@@ -1806,11 +1813,11 @@ struct ServeEngine {
         cudaError_t e = serve_occupancy(cfg.P, cfg.C, cfg.Hz, cfg.D, cfg.M, cfg.sup16, &occ);
         if (e != cudaSuccess) return e;
         if (occ < 1) return cudaErrorInvalidConfiguration;
-        L.ctas = std::max(sms * occ, SERVE_DEEP / cfg.D + 1);
+        L.ctas = std::max(sms * occ, n_deep / cfg.D + 1);
         // the overflow decoders' tile must hold this launch's top-z index
         args.deep_bytes = decoder_smem_bytes(cfg.deep_P, cfg.deep_C, cfg.Hz, 1, cfg.sup16);
         if (args.deep_bytes > deep_bytes()) return cudaErrorInvalidConfiguration;
-        h_word[2] = L.ctas * cfg.D - SERVE_DEEP;                  // main decoders
+        h_word[2] = L.ctas * cfg.D - n_deep;                      // main decoders
         send_stop(0);
         e = cudaMemcpyAsync(ctl + 7, h_word + 2, sizeof(int), cudaMemcpyHostToDevice, up);
         if (e == cudaSuccess) e = cudaEventRecord(ev_go, up);     // the launch follows every upload so far

@@ -1579,7 +1579,7 @@ __device__ __forceinline__ void decoder1_body(const DecoderArgs& a, unsigned cha
         }
         // a serving main decoder hands a restart that outgrew its tile to the
         // launch's overflow decoders instead of reporting it
-        const bool to_deep = MODE == 1 && (err == ERR_BOX_CAP || err == ERR_CAND_CAP);
+        const bool to_deep = MODE == 1 && sv.n_deep > 0 && (err == ERR_BOX_CAP || err == ERR_CAND_CAP);
         if (lane == 0 && !to_deep) {
             if (err) atomicOr(a.err_flag, 1 << err);
             SlotHead h;
