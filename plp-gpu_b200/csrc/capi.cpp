@@ -1541,6 +1541,15 @@ struct PinnedRing {
     }
 };
 
+// PLP_SERVE_TRACE=1: one stderr line per launch, stop and launch end
+bool serve_trace() {
+    static const bool on = [] {
+        const char* v = std::getenv("PLP_SERVE_TRACE");
+        return v && v[0] == '1';
+    }();
+    return on;
+}
+
 size_t serve_align(size_t x, size_t unit) {    // a multiple of unit and of 128 bytes
     size_t q = unit;
     while (q % 128) q += unit;
@@ -1712,10 +1721,13 @@ struct ServeEngine {
         cv.notify_all();
         if (th.joinable()) th.join();
         cudaSetDevice(device);
+        if (serve_trace()) std::fprintf(stderr, "[serve %.6f] teardown running=%d\n", now_seconds(), (int)running);
         if (running) {
             send_stop(1);
+            cudaStreamSynchronize(up);       // the stop word is in device memory
             cudaEventSynchronize(ev_kern);   // decoders finish their items and leave
         }
+        if (serve_trace()) std::fprintf(stderr, "[serve %.6f] teardown launch ended\n", now_seconds());
         for (cudaStream_t s : {up, kern, down})
             if (s) cudaStreamSynchronize(s);
         for (ServeJob* j : active) drop(j);
@@ -1741,9 +1753,17 @@ struct ServeEngine {
     // pinned constant: a copy runs on a copy engine while the serving launch
     // holds every SM, where a memset (which may run as a kernel) would wait
     // for the launch to end.
+    // The query submits the copy at once: work enqueued on a stream can wait
+    // in the driver until something flushes that stream, and a caller that
+    // then waits on the launch's stream alone would wait for the decoders'
+    // idle bound instead.
     void send_stop(int v) {
-        cudaMemcpyAsync(ctl + 2, h_word + (v ? 5 : 6), sizeof(int), cudaMemcpyHostToDevice, up);
+        const cudaError_t e = cudaMemcpyAsync(ctl + 2, h_word + (v ? 5 : 6), sizeof(int), cudaMemcpyHostToDevice, up);
+        (void)cudaStreamQuery(up);
         stop_sent = v != 0;
+        if (serve_trace())
+            std::fprintf(stderr, "[serve %.6f] stop=%d (%s) running=%d\n", now_seconds(), v, cudaGetErrorString(e),
+                         (int)running);
     }
 
     bool allocate(ServeJob& j) {
@@ -1830,6 +1850,9 @@ struct ServeEngine {
             running = true;
             n_launches++;
         }
+        if (serve_trace())
+            std::fprintf(stderr, "[serve %.6f] launch ctas=%d P=%d C=%d Hz=%d sup16=%d deep=%d tail=%d (%s)\n",
+                         now_seconds(), L.ctas, cfg.P, cfg.C, cfg.Hz, cfg.sup16, n_deep, tail, cudaGetErrorString(e));
         return e;
     }
 
@@ -1881,6 +1904,7 @@ struct ServeEngine {
         if (e == cudaSuccess) e = cudaEventRecord(j.ev_up, up);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&j.ev, cudaEventDisableTiming);
         if (e != cudaSuccess) return set_cuda_error("serving upload", e);
+        (void)cudaStreamQuery(up);     // submit now: the running launch is waiting for the tail
         published += R;
         return PLP_OK;
     }
@@ -1890,6 +1914,7 @@ struct ServeEngine {
     void fallback(ServeJob& j) {
         if (running) {                 // the serving launch holds the SMs: let it finish its items
             send_stop(1);
+            cudaStreamSynchronize(up);
             cudaEventSynchronize(ev_kern);
             running = false;
         }
@@ -2065,6 +2090,9 @@ struct ServeEngine {
         if (running && cudaEventQuery(ev_kern) == cudaSuccess) {
             running = false;
             progress = true;
+            if (serve_trace())
+                std::fprintf(stderr, "[serve %.6f] launch ended head=%d overflow=%d/%d tail=%d\n", now_seconds(),
+                             h_word[0], h_word[3], h_word[4], tail);
         }
         if (!running && !broken && work_left()) {
             const cudaError_t e = launch();
