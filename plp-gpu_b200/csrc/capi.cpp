@@ -2532,14 +2532,21 @@ int plp_create(size_t budget_bytes, int32_t device, plp_handle** out) {
 
 void plp_destroy(plp_handle* h) {
     if (!h) return;
+    // The serving launch goes first: a worker frees its pinned buffers as it
+    // exits, and a pinned free waits for every kernel on the device, the
+    // serving launch included, which would run on to its idle bound.
+    {
+        std::lock_guard<std::mutex> g(h->serve_mu);
+        delete h->serve;          // stops its launch and thread
+        h->serve = nullptr;
+        h->serve_off = true;
+    }
     {
         std::lock_guard<std::mutex> lk(h->mu);
         h->stop = true;
     }
     h->cv_sched.notify_all();
     for (auto& t : h->workers) t.join();
-    delete h->serve;              // stops its launch and thread
-    h->serve = nullptr;
     for (auto& kv : h->reqs) delete kv.second->result;
     for (auto s : h->streams) cudaStreamDestroy(s);
     if (h->sync_stream) cudaStreamDestroy(h->sync_stream);
