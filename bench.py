@@ -574,7 +574,9 @@ def main():
         tile = tuple(int(v) for v in args.tile.split(","))
         h.set_tile(*tile)
     else:
-        tile = h.autotune(insts, opts)
+        # a sample of up to 1/8 of the workload (at least the tuner's default
+        # 32768 decodes) keeps the estimates' spread below the tiles' gaps
+        tile = h.autotune(insts, opts, max_decodes=max(32768, R * len(insts) // 8))
 
     # ---- device-resident timing (value) ----
     batch = h.prepare(insts, opts)
