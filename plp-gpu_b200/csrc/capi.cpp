@@ -2645,7 +2645,7 @@ int plp_autotune(plp_handle* h, const plp_instance* const* insts, int32_t n_inst
     for (int p : {64, 128, 256})
         if (p <= P_MAX && (p >= std::min(max_steps, 64) || p == 128)) Ps.push_back(p);
     for (int c : {256, 384, 512, 768}) Cs.push_back(c);
-    const int dm[][2] = {{1, 1}, {1, 12}, {2, 1}, {4, 1}, {8, 1}, {8, 2}};
+    const int dm[][2] = {{1, 1}, {1, 12}, {1, 16}, {2, 1}, {4, 1}, {8, 1}, {8, 2}};
     std::vector<TileConfig> cand;
     for (int p : Ps)
         for (int c : Cs)

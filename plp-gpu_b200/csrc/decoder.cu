@@ -1800,7 +1800,7 @@ __global__ void gather_best_kernel(const InstDesc* __restrict__ inst, int n_inst
 // (G warps per decoder, D decoders per CTA, M minimum resident CTAs per SM:
 // a register cap of 65536 / (32 G D M) per thread) instantiations
 #define PLP_DECODER_CONFIGS(X)                                                                 \
-    X(1, 1, 1) X(1, 1, 12) X(1, 2, 1) X(1, 4, 1) X(1, 4, 4) X(1, 8, 1) X(1, 8, 2) X(2, 1, 1) X(2, 2, 1) X(2, 2, 5) \
+    X(1, 1, 1) X(1, 1, 12) X(1, 1, 16) X(1, 2, 1) X(1, 4, 1) X(1, 4, 4) X(1, 8, 1) X(1, 8, 2) X(2, 1, 1) X(2, 2, 1) X(2, 2, 5) \
     X(2, 4, 1) X(2, 4, 3) X(4, 1, 1) X(4, 1, 5) X(4, 1, 6) X(4, 2, 1) X(4, 2, 3) X(4, 4, 1)   \
     X(8, 1, 1) X(8, 1, 3) X(8, 2, 1)
 

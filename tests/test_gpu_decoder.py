@@ -109,7 +109,7 @@ def test_plain_path_matches_oracle(kw):
         assert O.strip_time(r.json(k)) == O.strip_time(js)
 
 
-CONFIGS = [(1, 1, 1), (1, 1, 12), (1, 2, 1), (1, 4, 1), (1, 4, 4), (1, 8, 1), (1, 8, 2), (2, 1, 1), (2, 2, 1), (2, 2, 5), (2, 4, 1),
+CONFIGS = [(1, 1, 1), (1, 1, 12), (1, 1, 16), (1, 2, 1), (1, 4, 1), (1, 4, 4), (1, 8, 1), (1, 8, 2), (2, 1, 1), (2, 2, 1), (2, 2, 5), (2, 4, 1),
            (2, 4, 3), (4, 1, 1), (4, 1, 5), (4, 1, 6), (4, 2, 1), (4, 2, 3), (4, 4, 1), (8, 1, 1), (8, 1, 3),
            (8, 2, 1)]
 
