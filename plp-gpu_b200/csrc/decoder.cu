@@ -147,9 +147,11 @@ __host__ __device__ inline Dec1Layout dec1_layout(int P, int C, int Hz, int sb) 
     return l;
 }
 
+#ifndef PLP_SERVE_TU
 int decoder_smem_bytes(int P, int C, int Hz, int G, int sup16) {
     return G == 1 ? dec1_layout(P, C, Hz, sup16 ? 2 : 4).bytes : dec_layout(P, C, Hz).bytes;
 }
+#endif
 
 struct DecoderArgs {
     const InstDesc* __restrict__ inst;
@@ -1379,10 +1381,10 @@ __device__ __forceinline__ void decoder1_body(const DecoderArgs& a, unsigned cha
     for (;;) {
         if (*reinterpret_cast<volatile int*>(a.abort)) break;
         int2 wk;
-        if (SERVE) {
+        if constexpr (SERVE) {
             int item = -1, wx = 0, wy = 0;
             if (lane == 0) {
-                if (MODE == 1) {
+                if constexpr (MODE == 1) {
                     item = serve_claim(sv);
                     if (item >= 0) {
                         const int2 w = ld_relaxed_gpu_int2(sv.ring + (item & sv.ring_mask));
@@ -1579,7 +1581,8 @@ __device__ __forceinline__ void decoder1_body(const DecoderArgs& a, unsigned cha
         }
         // a serving main decoder hands a restart that outgrew its tile to the
         // launch's overflow decoders instead of reporting it
-        const bool to_deep = MODE == 1 && sv.n_deep > 0 && (err == ERR_BOX_CAP || err == ERR_CAND_CAP);
+        bool to_deep = false;
+        if constexpr (MODE == 1) to_deep = sv.n_deep > 0 && (err == ERR_BOX_CAP || err == ERR_CAND_CAP);
         if (lane == 0 && !to_deep) {
             if (err) atomicOr(a.err_flag, 1 << err);
             SlotHead h;
@@ -1592,15 +1595,46 @@ __device__ __forceinline__ void decoder1_body(const DecoderArgs& a, unsigned cha
             a.heads[slot] = h;
         }
         __syncwarp();
-        if (to_deep) serve_push_deep(sv, wk, lane);
-        else if (SERVE) serve_finish(a, sv, wk.x, I, lane);
+        if constexpr (SERVE) {
+            if (to_deep) serve_push_deep(sv, wk, lane);
+            else serve_finish(a, sv, wk.x, I, lane);
+        }
     }
-    if (MODE == 1 && lane == 0) {   // pushes above are visible before the count drops
-        __threadfence();
-        atomicSub(sv.alive, 1);
+    if constexpr (MODE == 1) {
+        if (lane == 0) {   // pushes above are visible before the count drops
+            __threadfence();
+            atomicSub(sv.alive, 1);
+        }
     }
 }
 
+static DecoderArgs decoder_args(const DecodeLaunch& L) {
+    DecoderArgs a;
+    a.inst = L.inst;
+    a.step_type = L.step_type;
+    a.types = L.types;
+    a.work = L.work;
+    a.n_work = L.n_work;
+    a.n_work_dev = L.n_work_dev;
+    a.work_next = L.work_next;
+    a.err_flag = L.err_flag;
+    a.abort = L.abort;
+    a.heads = L.heads;
+    a.places = L.places;
+    a.scratch = L.scratch;
+    a.mt_init = L.mt_init;
+    a.P = L.P;
+    a.C = L.C;
+    a.Hz = L.Hz;
+    a.sync_limit = L.sync_limit;
+    a.sync_skip = L.sync_skip;
+    a.seed_tab = L.seed_tab;
+    a.seed_lo = L.seed_lo;
+    a.seed_n = L.seed_n;
+    return a;
+}
+
+#ifndef PLP_SERVE_TU
 // S16: contact areas stored as 16-bit (every footprint area < 65536)
 template <int D, int M, int S16>
 __global__ void __launch_bounds__(32 * D, M) decoder1_kernel(DecoderArgs a) {
@@ -1611,23 +1645,6 @@ __global__ void __launch_bounds__(32 * D, M) decoder1_kernel(DecoderArgs a) {
     decoder1_body<SupT, 0>(a, smem_raw + (size_t)dec * lay.bytes, blockIdx.x * D + dec, ServeArgs{});
 }
 
-// The serving launch: the single-warp decoder over the host-published ring.
-template <int D, int M, int S16>
-__global__ void __launch_bounds__(32 * D, M) serve_kernel(DecoderArgs a, ServeArgs s) {
-    using SupT = typename std::conditional<S16 != 0, unsigned short, int>::type;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int dec = threadIdx.x >> 5;
-    const int gdec = blockIdx.x * D + dec;
-    if (gdec < s.n_deep) {
-        DecoderArgs ad = a;
-        ad.P = s.deep_P;
-        ad.C = s.deep_C;
-        decoder1_body<SupT, 2>(ad, s.deep_scratch + (size_t)gdec * s.deep_bytes, gdec, s);
-    } else {
-        const Dec1Layout lay = dec1_layout(a.P, a.C, a.Hz, (int)sizeof(SupT));
-        decoder1_body<SupT, 1>(a, smem_raw + (size_t)dec * lay.bytes, gdec, s);
-    }
-}
 
 // ---------------------------------------------------------------------------
 // per-instance best restart: accepted first, then max (volume, n_boxes),
@@ -1863,31 +1880,6 @@ cudaError_t cached_occupancy(const void* fn, int threads, int smem, int* ctas_pe
     return cudaSuccess;
 }
 
-static DecoderArgs decoder_args(const DecodeLaunch& L) {
-    DecoderArgs a;
-    a.inst = L.inst;
-    a.step_type = L.step_type;
-    a.types = L.types;
-    a.work = L.work;
-    a.n_work = L.n_work;
-    a.n_work_dev = L.n_work_dev;
-    a.work_next = L.work_next;
-    a.err_flag = L.err_flag;
-    a.abort = L.abort;
-    a.heads = L.heads;
-    a.places = L.places;
-    a.scratch = L.scratch;
-    a.mt_init = L.mt_init;
-    a.P = L.P;
-    a.C = L.C;
-    a.Hz = L.Hz;
-    a.sync_limit = L.sync_limit;
-    a.sync_skip = L.sync_skip;
-    a.seed_tab = L.seed_tab;
-    a.seed_lo = L.seed_lo;
-    a.seed_n = L.seed_n;
-    return a;
-}
 
 static int decoder_launch_smem(const DecodeLaunch& L) {
     return decoder_smem_bytes(L.P, L.C, L.Hz, L.warps_per_decoder, L.sup16) * L.decoders_per_cta;
@@ -1924,41 +1916,6 @@ cudaError_t launch_decoder(const DecodeLaunch& L, cudaStream_t st) {
 cudaError_t launch_seed_table(long long lo, int n, const uint32_t* mt_init, uint32_t* out, cudaStream_t st) {
     if (n <= 0) return cudaSuccess;
     seed_table_kernel<<<(n + 3) / 4, 128, 0, st>>>(lo, n, mt_init, out);
-    return cudaGetLastError();
-}
-
-// ---- serving launches ------------------------------------------------------
-using ServeFn = void (*)(DecoderArgs, ServeArgs);
-#define PLP_SERVE_CONFIGS(X) X(1, 1) X(1, 12)
-
-static ServeFn serve_fn(int D, int M, int sup16) {
-#define PLP_PICK_SERVE(d, m) \
-    if (D == d && M == m) return sup16 ? serve_kernel<d, m, 1> : serve_kernel<d, m, 0>;
-    PLP_SERVE_CONFIGS(PLP_PICK_SERVE)
-#undef PLP_PICK_SERVE
-    return nullptr;
-}
-
-bool serve_config_supported(int D, int M) { return serve_fn(D, M, 0) != nullptr; }
-
-cudaError_t serve_occupancy(int P, int C, int Hz, int D, int M, int sup16, int* ctas_per_sm) {
-    ServeFn fn = serve_fn(D, M, sup16);
-    if (!fn) return cudaErrorInvalidConfiguration;
-    const int smem = decoder_smem_bytes(P, C, Hz, 1, sup16) * D;
-    cudaError_t e = ensure_dyn_smem(reinterpret_cast<const void*>(fn), smem);
-    if (e != cudaSuccess) return e;
-    return cached_occupancy(reinterpret_cast<const void*>(fn), 32 * D, smem, ctas_per_sm);
-}
-
-cudaError_t launch_serve(const DecodeLaunch& L, const ServeArgs& s, cudaStream_t st) {
-    ServeFn fn = serve_fn(L.decoders_per_cta, L.min_blocks, L.sup16);
-    if (!fn || L.warps_per_decoder != 1 || L.engine != 0) return cudaErrorInvalidConfiguration;
-    const int smem = decoder_smem_bytes(L.P, L.C, L.Hz, 1, L.sup16) * L.decoders_per_cta;
-    cudaError_t e = ensure_dyn_smem(reinterpret_cast<const void*>(fn), smem);
-    if (e != cudaSuccess) return e;
-    e = cudaMemsetAsync(L.abort, 0, sizeof(int), st);
-    if (e != cudaSuccess) return e;
-    fn<<<L.ctas, 32 * L.decoders_per_cta, smem, st>>>(decoder_args(L), s);
     return cudaGetLastError();
 }
 
@@ -2039,5 +1996,63 @@ cudaError_t launch_gather_best(const InstDesc* inst, int n_inst, const int2* bes
                                                                      out_stride);
     return cudaGetLastError();
 }
+
+#endif  // PLP_SERVE_TU
+
+#ifdef PLP_SERVE_TU
+// The serving launch: the single-warp decoder over the host-published ring.
+template <int D, int M, int S16>
+__global__ void __launch_bounds__(32 * D, M) serve_kernel(DecoderArgs a, ServeArgs s) {
+    using SupT = typename std::conditional<S16 != 0, unsigned short, int>::type;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int dec = threadIdx.x >> 5;
+    const int gdec = blockIdx.x * D + dec;
+    if (gdec < s.n_deep) {
+        DecoderArgs ad = a;
+        ad.P = s.deep_P;
+        ad.C = s.deep_C;
+        decoder1_body<SupT, 2>(ad, s.deep_scratch + (size_t)gdec * s.deep_bytes, gdec, s);
+    } else {
+        const Dec1Layout lay = dec1_layout(a.P, a.C, a.Hz, (int)sizeof(SupT));
+        decoder1_body<SupT, 1>(a, smem_raw + (size_t)dec * lay.bytes, gdec, s);
+    }
+}
+
+// ---- serving launches ------------------------------------------------------
+using ServeFn = void (*)(DecoderArgs, ServeArgs);
+#define PLP_SERVE_CONFIGS(X) X(1, 1) X(1, 12)
+
+static ServeFn serve_fn(int D, int M, int sup16) {
+#define PLP_PICK_SERVE(d, m) \
+    if (D == d && M == m) return sup16 ? serve_kernel<d, m, 1> : serve_kernel<d, m, 0>;
+    PLP_SERVE_CONFIGS(PLP_PICK_SERVE)
+#undef PLP_PICK_SERVE
+    return nullptr;
+}
+
+bool serve_config_supported(int D, int M) { return serve_fn(D, M, 0) != nullptr; }
+
+cudaError_t serve_occupancy(int P, int C, int Hz, int D, int M, int sup16, int* ctas_per_sm) {
+    ServeFn fn = serve_fn(D, M, sup16);
+    if (!fn) return cudaErrorInvalidConfiguration;
+    const int smem = decoder_smem_bytes(P, C, Hz, 1, sup16) * D;
+    cudaError_t e = ensure_dyn_smem(reinterpret_cast<const void*>(fn), smem);
+    if (e != cudaSuccess) return e;
+    return cached_occupancy(reinterpret_cast<const void*>(fn), 32 * D, smem, ctas_per_sm);
+}
+
+cudaError_t launch_serve(const DecodeLaunch& L, const ServeArgs& s, cudaStream_t st) {
+    ServeFn fn = serve_fn(L.decoders_per_cta, L.min_blocks, L.sup16);
+    if (!fn || L.warps_per_decoder != 1 || L.engine != 0) return cudaErrorInvalidConfiguration;
+    const int smem = decoder_smem_bytes(L.P, L.C, L.Hz, 1, L.sup16) * L.decoders_per_cta;
+    cudaError_t e = ensure_dyn_smem(reinterpret_cast<const void*>(fn), smem);
+    if (e != cudaSuccess) return e;
+    e = cudaMemsetAsync(L.abort, 0, sizeof(int), st);
+    if (e != cudaSuccess) return e;
+    fn<<<L.ctas, 32 * L.decoders_per_cta, smem, st>>>(decoder_args(L), s);
+    return cudaGetLastError();
+}
+
+#endif  // PLP_SERVE_TU
 
 }  // namespace plpb
