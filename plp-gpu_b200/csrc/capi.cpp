@@ -10,6 +10,7 @@
 #include <chrono>
 #include <climits>
 #include <condition_variable>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <deque>
@@ -1663,6 +1664,16 @@ struct ServeEngine {
         if (e == cudaSuccess) e = cudaMalloc(&ring, sizeof(int2) * SERVE_RING);
         if (e == cudaSuccess) e = cudaMalloc(&dring, sizeof(int4) * SERVE_RING);
         if (e == cudaSuccess) e = cudaMemset(dring, 0, sizeof(int4) * SERVE_RING);
+        // PLP_SERVE_TILE=P,C,M: the main decoders' tile (M 1 or 12)
+        if (const char* v = std::getenv("PLP_SERVE_TILE")) {
+            int p = 0, c = 0, m = 0;
+            if (std::sscanf(v, "%d,%d,%d", &p, &c, &m) == 3 && p >= 16 && p <= P_MAX && c >= 32 && c <= C_MAX &&
+                c % 32 == 0 && serve_config_supported(1, m)) {
+                cfg.P = p;
+                cfg.C = c;
+                cfg.M = m;
+            }
+        }
         n_deep = SERVE_DEEP;
         if (const char* v = std::getenv("PLP_SERVE_DEEP")) {
             char* end = nullptr;
