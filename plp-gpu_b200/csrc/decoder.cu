@@ -1454,12 +1454,17 @@ __device__ __forceinline__ void decoder1_body(const DecoderArgs& a, unsigned cha
             __syncwarp();
             int state_type = -1;
             bool pending = false;   // a placed box not yet applied to the valid states
+            bool stuck = false;     // the last step of state_type found no feasible pair
             int4 B = make_int4(0, 0, 0, 0);
             int Bz = 0, Bz2 = 0;
             int t_next = I.n_steps > 0 ? ld_table<SERVE>(a.step_type + I.step_off) : 0;
             for (int sti = 0; sti < I.n_steps; sti++) {
                 const int t = t_next;
                 if (sti + 1 < I.n_steps) t_next = ld_table<SERVE>(a.step_type + I.step_off + sti + 1);
+                // With no box placed since, another item of that type meets the
+                // same states and finds no pair either; it draws no random
+                // number, so the step is skipped without changing the result.
+                if (stuck && t == state_type) continue;
                 const TypeOrs& T = a.types[I.type_off + t];
                 StepOrs S;
                 S.no = ld_table<SERVE>(&T.n);
@@ -1552,7 +1557,8 @@ __device__ __forceinline__ void decoder1_body(const DecoderArgs& a, unsigned cha
                     greedy = false;   // every feasible pair is needed
                     hi = nW;
                 }
-                if (pp == INT_MAX) continue;             // no feasible pair: no draw
+                stuck = pp == INT_MAX;
+                if (stuck) continue;                     // no feasible pair: no draw
                 err = place1(t, pp, full, mt, mpos, keys, st, sup, bx, bzs, z2s, bis, zt, a.Hz, nc, nb, a.P,
                              C, S, xmask, ymask, xb, xyb, pass_out, vol, B, Bz, Bz2, lane);
                 if (err != ERR_NONE) break;
