@@ -349,10 +349,11 @@ __device__ __forceinline__ void scan_points(DecShared* sh, const uint2* W, unsig
             for (int u = 0; u < 4; u++) {
                 if ((todo >> u) & 1u) {                 // uniform: some lane is near box u
                     if ((near >> u) & 1u) {
-                        const int4 b = bb[u];
+                        // offsets from the point (coordinates are below 2^16)
+                        const int dx = bb[u].x - x, dy = bb[u].y - y, dz = bz[u] - z;
 #pragma unroll
                         for (int o = 0; o < 6; o++)
-                            if (b.x < x + S.ow[o] && b.y < y + S.od[o] && bz[u] < z + S.oh[o]) alive &= ~(1u << o);
+                            if (dx < S.ow[o] && dy < S.od[o] && dz < S.oh[o]) alive &= ~(1u << o);
                     }
                 }
             }
@@ -901,10 +902,11 @@ __device__ __forceinline__ int2 eval_items(const bool GREEDY, const uint2* W, co
             for (int u = 0; u < 4; u++) {
                 if ((todo >> u) & 1u) {
                     if ((near >> u) & 1u) {
-                        const int4 b = bb[u];
+                        // offsets from the point (coordinates are below 2^16)
+                        const int dx = bb[u].x - x, dy = bb[u].y - y, dz = bz[u] - z;
 #pragma unroll
                         for (int o = 0; o < 6; o++)
-                            if (b.x < x + S.ow[o] && b.y < y + S.od[o] && bz[u] < z + S.oh[o]) alive &= ~(1u << o);
+                            if (dx < S.ow[o] && dy < S.od[o] && dz < S.oh[o]) alive &= ~(1u << o);
                     }
                 }
             }
@@ -942,14 +944,18 @@ __device__ __forceinline__ int2 eval_items(const bool GREEDY, const uint2* W, co
 template <typename SupT>
 __device__ __forceinline__ uint32_t st_apply_box(uint32_t s, int x, int y, int z, int4 B, int Bz, int Bz2,
                                                  const StepOrs& S, SupT* sup, int C, int p) {
+    const bool above = Bz2 > z && x < B.z && y < B.w;
+    const bool level = z > 0 && Bz2 == z;
+    if (!above && !level) return s;   // the box neither blocks nor supports the point
     const unsigned m2 = s & 0x3fu, known = (s >> 24) & 0x3fu;
     unsigned blk = (s >> 8) & 0x3fu, sok = (s >> 16) & 0x3fu;
-    if (Bz2 > z && x < B.z && y < B.w) {
+    if (above) {
+        const int dx = B.x - x, dy = B.y - y, dz = Bz - z;
 #pragma unroll
         for (int o = 0; o < 6; o++)
-            if (B.x < x + S.ow[o] && B.y < y + S.od[o] && Bz < z + S.oh[o]) blk |= 1u << o;
+            if (dx < S.ow[o] && dy < S.od[o] && dz < S.oh[o]) blk |= 1u << o;
     }
-    if (z > 0 && Bz2 == z) {
+    if (level) {
 #pragma unroll
         for (int o = 0; o < 6; o++) {
             if ((m2 >> o) & 1u) {
