@@ -279,3 +279,36 @@ def test_multi_restart_every_one_of_1024_restarts_and_best_match_reference_host(
     assert row == g["best"]["row"]
     accepted = [e for e in g["restarts"] if e[3] >= 0.9] or g["restarts"]
     assert row["volume_cm3"] == max(e[1] for e in accepted)
+
+
+# A 12-cube that fits once and a 9-cube that never fits in a 20-cube
+# container: their items fail step after step with nothing placed in
+# between, which the decoder skips (a repeat of a failed type meets the same
+# states and draws no random number). The 4-cubes and bars after them must
+# come out as the oracle places them.
+REPEATED_FAILURES = ("1\n1 7\n20 20 20\n4\n1 12 1 12 1 12 1 6\n2 9 1 9 1 9 1 10\n"
+                     "3 4 1 4 1 4 1 40\n4 13 1 2 1 2 1 3\n")
+
+
+@pytest.mark.parametrize("passes", [1, 2])
+def test_repeated_failures_of_a_type_match_oracle(handle, passes):
+    inst = P.Instance.parse(REPEATED_FAILURES)
+    oi = O.OInstance(REPEATED_FAILURES)
+    res = handle.solve([inst], P.make_opts(seed=3, restarts=8, passes=passes, eps=0.5))[0]
+    for k in range(8):
+        js, _, _ = O.run(oi, seed=3 + k, passes=passes, eps=0.5)
+        assert O.strip_time(res.json(k)) == O.strip_time(js), k
+
+
+def test_repeated_failures_of_a_type_served_match_oracle():
+    """The same instance through the serving launch (its main decoders share
+    the decoder body)."""
+    inst = P.Instance.parse(REPEATED_FAILURES)
+    oi = O.OInstance(REPEATED_FAILURES)
+    with P.Handle() as h:
+        rid = h.submit(inst, P.make_opts(seed=11, restarts=16, eps=0.5))
+        assert h.wait(rid, 600000) == P.OK
+        res = h.take(rid)
+    for k in range(16):
+        js, _, _ = O.run(oi, seed=11 + k, eps=0.5)
+        assert O.strip_time(res.json(k)) == O.strip_time(js), k
