@@ -1664,11 +1664,13 @@ struct ServeEngine {
         if (e == cudaSuccess) e = cudaMalloc(&ring, sizeof(int2) * SERVE_RING);
         if (e == cudaSuccess) e = cudaMalloc(&dring, sizeof(int4) * SERVE_RING);
         if (e == cudaSuccess) e = cudaMemset(dring, 0, sizeof(int4) * SERVE_RING);
-        // PLP_SERVE_TILE=P,C,M: the main decoders' tile (M 1 or 12)
+        // PLP_SERVE_TILE=P,C,M: the main decoders' tile (M 1 or 12); taken
+        // only if it fits one CTA's shared memory with the largest top-z
+        // index and 32-bit contact areas, so no later launch can fail on it
         if (const char* v = std::getenv("PLP_SERVE_TILE")) {
             int p = 0, c = 0, m = 0;
             if (std::sscanf(v, "%d,%d,%d", &p, &c, &m) == 3 && p >= 16 && p <= P_MAX && c >= 32 && c <= C_MAX &&
-                c % 32 == 0 && serve_config_supported(1, m)) {
+                c % 32 == 0 && serve_config_supported(1, m) && decoder_smem_bytes(p, c, 4096, 1, 0) <= 227 * 1024) {
                 cfg.P = p;
                 cfg.C = c;
                 cfg.M = m;
