@@ -320,6 +320,23 @@ int build_block_tables(const Instance& I, const std::vector<TypeOrs>& ors, const
     return PLP_OK;
 }
 
+// Orientation table of every box type of an instance; clears *small when an
+// orientation's footprint area reaches 65536 (its contact areas need 32 bits).
+std::vector<TypeOrs> type_orientations(const Instance& I, int* small) {
+    std::vector<TypeOrs> ot;
+    ot.reserve(I.types.size());
+    for (const auto& t : I.types) {
+        TypeOrs to{};
+        const auto v = orientations(t);
+        to.n = (int)v.size();
+        for (int k = 0; k < to.n; k++) { to.w[k] = v[k][0]; to.d[k] = v[k][1]; to.h[k] = v[k][2]; }
+        for (int k = 0; k < to.n; k++)
+            if (1LL * to.w[k] * to.d[k] >= 65536) *small = 0;
+        ot.push_back(to);
+    }
+    return ot;
+}
+
 struct Batch {
     std::vector<const Instance*> insts;
     std::vector<plp_run_opts> opts;
@@ -391,23 +408,40 @@ struct Batch {
         n_slots = 0; n_places = 0; max_stride = 1; max_steps = 0; multi_pass = false;
         int maxH = 0;
         best_only = true;
-        // item sequences of a large batch are sorted on several threads; the
-        // rest of the build is appends in instance order
+        // item sequences and orientation tables of a large batch are built on
+        // several threads; the rest of the build is appends in instance order
         std::vector<std::vector<int>> seqs;
+        std::vector<std::vector<TypeOrs>> ors;
+        std::vector<int> ors_small;
         if (in.size() >= 256) {
             seqs.resize(in.size());
+            ors.resize(in.size());
+            ors_small.assign(in.size(), 1);
             const unsigned hw = std::thread::hardware_concurrency();
             const int nt = (int)std::max(1u, std::min(16u, hw ? hw : 1u));
             std::atomic<size_t> next{0};
             auto job = [&] {
                 for (size_t i0; (i0 = next.fetch_add(64)) < in.size();)
-                    for (size_t k = i0; k < std::min(in.size(), i0 + 64); k++)
+                    for (size_t k = i0; k < std::min(in.size(), i0 + 64); k++) {
                         if (op[k].order == 0 || op[k].order == 1) seqs[k] = item_sequence(*in[k], op[k].order);
+                        ors[k] = type_orientations(*in[k], &ors_small[k]);
+                    }
             };
             std::vector<std::thread> pool;
             for (int t = 1; t < nt; t++) pool.emplace_back(job);
             job();
             for (auto& th : pool) th.join();
+        }
+        {
+            size_t n_types = 0, n_steps = 0;
+            for (size_t i = 0; i < in.size(); i++) {
+                n_types += in[i]->types.size();
+                if (!seqs.empty()) n_steps += seqs[i].size();
+            }
+            desc.reserve(in.size());
+            inst_ors.reserve(in.size());
+            types.reserve(n_types);
+            steps.reserve(n_steps);
         }
         for (size_t i = 0; i < in.size(); i++) {
             const Instance& I = *in[i];
@@ -454,17 +488,16 @@ struct Batch {
             d.first_fit = o.first_fit ? 1 : 0;
             desc.push_back(d);
             steps.insert(steps.end(), seq.begin(), seq.end());
+            int small = 1;
             std::vector<TypeOrs> ot;
-            for (const auto& t : I.types) {
-                TypeOrs to{};
-                const auto v = orientations(t);
-                to.n = (int)v.size();
-                for (int k = 0; k < to.n; k++) { to.w[k] = v[k][0]; to.d[k] = v[k][1]; to.h[k] = v[k][2]; }
-                for (int k = 0; k < to.n; k++)
-                    if (1LL * to.w[k] * to.d[k] >= 65536) sup16_ok = 0;
-                ot.push_back(to);
-                types.push_back(to);
+            if (ors.empty()) {
+                ot = type_orientations(I, &small);
+            } else {
+                ot = std::move(ors[i]);
+                small = ors_small[i];
             }
+            if (!small) sup16_ok = 0;
+            types.insert(types.end(), ot.begin(), ot.end());
             desc.back().engine = o.engine;
             desc.back().n_types = (int)I.types.size();
             max_types = std::max(max_types, (int)I.types.size());
